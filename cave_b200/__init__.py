@@ -1,0 +1,231 @@
+"""cave_b200 -- B200 (sm_100a) CA stepping for CAVE's search path, Python binding.
+
+Thin ctypes binding over ``libcave_ca.so`` (the C ABI declared in ``include/cave_ca.h``).
+All computation happens in the library's CUDA kernels; this module only marshals arguments.
+If the shared library is missing the import of any entry point raises -- there is no CPU
+fallback in the product.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcave_ca.so")
+HEADER_PATH = os.path.join(_HERE, "..", "include", "cave_ca.h")
+
+PERM_MASK = (1 << 60) - 1
+
+OK, ERR_INVALID_ARG, ERR_CUDA, ERR_OUT_OF_MEMORY, ERR_NOT_READY, ERR_TIMEOUT, ERR_IO, ERR_INTERNAL = range(8)
+
+u8, u32, u64, i32, sz = ctypes.c_uint8, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int, ctypes.c_size_t
+P = ctypes.POINTER
+
+
+class SimParams(ctypes.Structure):
+    _fields_ = [("birthAndMaxCellStateRules", u64), ("survivalAndNeighborhoodRules", u64),
+                ("shapeAndGridConfiguration", u64)]
+
+
+class GridSnapshot(ctypes.Structure):
+    _fields_ = [("numberOfDeadCells", u32), ("numberOfDyingCells", u32), ("numberOfCellsBorn", u32),
+                ("numberOfSurvivingCells", u32)]
+
+    def as_tuple(self):
+        return (self.numberOfDeadCells, self.numberOfDyingCells, self.numberOfCellsBorn, self.numberOfSurvivingCells)
+
+
+class GridInfo(ctypes.Structure):
+    _fields_ = [("totalNumberOfCellsThatDied", u32), ("totalNumberOfCellsThatWereBorn", u32),
+                ("numberOfSimulationTicksSurvived", u32), ("status", u32), ("maxAliveCount", u32),
+                ("finalAliveCount", u32)]
+
+    def as_tuple(self):
+        return (self.totalNumberOfCellsThatDied, self.totalNumberOfCellsThatWereBorn,
+                self.numberOfSimulationTicksSurvived, self.status, self.maxAliveCount, self.finalAliveCount)
+
+
+class ChunkConfig(ctypes.Structure):
+    _fields_ = [(n, u32) for n in (
+        "shapeId", "gridDimensionX", "gridDimensionY", "gridDimensionZ", "spawnAreaDimensionX",
+        "spawnAreaDimensionY", "spawnAreaDimensionZ", "spawnPlacementId", "spawnRegionShapeId", "spawnSizeIndex",
+        "spawnDensityIndex", "runSeedIndex", "partitionIndex", "partitionCount")]
+
+
+class TickStats(ctypes.Structure):
+    _fields_ = [("snapshot", GridSnapshot), ("population", u32), ("changed", u32), ("bbox_min", u32 * 3),
+                ("bbox_max", u32 * 3)]
+
+    def as_tuple(self):
+        return self.snapshot.as_tuple() + (self.population, self.changed, tuple(self.bbox_min),
+                                           tuple(self.bbox_max))
+
+
+class CaveError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{msg} (status {code})")
+        self.code = code
+
+
+_lib = None
+
+# name -> (restype, argtypes); every entry point of include/cave_ca.h
+_SIGS = {
+    "cave_ctx_create": (i32, [i32, P(ctypes.c_void_p)]),
+    "cave_ctx_destroy": (None, [ctypes.c_void_p]),
+    "cave_status_string": (ctypes.c_char_p, [i32]),
+    "cave_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "cave_ctx_synchronize": (i32, [ctypes.c_void_p]),
+    "cave_grid_create": (i32, [ctypes.c_void_p, u32, u32, u32, P(ctypes.c_void_p)]),
+    "cave_grid_destroy": (None, [ctypes.c_void_p]),
+    "cave_grid_words": (u64, [u32, u32, u32]),
+    "cave_grid_upload": (i32, [ctypes.c_void_p, P(u32), u64]),
+    "cave_grid_download": (i32, [ctypes.c_void_p, P(u32), u64]),
+    "cave_grid_seed": (i32, [ctypes.c_void_p, P(ChunkConfig), u32]),
+    "cave_grid_seed_threshold": (i32, [ctypes.c_void_p, u32, u32, u32, u64, u32, u32]),
+    "cave_step": (i32, [ctypes.c_void_p, P(SimParams), P(u64), u32, u32, u32, P(TickStats)]),
+    "cave_run": (i32, [ctypes.c_void_p, P(SimParams), P(u64), u32, u32, u32, u32, P(TickStats), P(GridInfo)]),
+    "cave_manager_update": (None, [P(GridSnapshot), P(GridInfo), P(SimParams), u64, u64, u32, P(GridInfo),
+                                   P(SimParams)]),
+    "cave_enumerate_valid_bitmasks": (u64, [u32, u32, P(u64), u64]),
+}
+
+
+def lib():
+    """Loads libcave_ca.so (raises OSError if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is missing: run `python -m cave_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _u32p(a):
+    assert a.dtype == np.uint32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(P(u32))
+
+
+def _u64p(a):
+    if a is None:
+        return None
+    assert a.dtype == np.uint64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(P(u64))
+
+
+def make_params(max_cell_state, flags, birth, survival, shape_id=0) -> SimParams:
+    """SimulationParameters with the simulation.h:58 maxCellState encoding."""
+    return SimParams((((max_cell_state - 1) & 0xF) << 60) | (birth & PERM_MASK),
+                     ((flags & 0xF) << 60) | (survival & PERM_MASK), shape_id & 0x1F)
+
+
+def grid_words(X, Y, Z) -> int:
+    return int(lib().cave_grid_words(X, Y, Z))
+
+
+def valid_bitmasks(neighbor_count, max_bits) -> np.ndarray:
+    n = lib().cave_enumerate_valid_bitmasks(neighbor_count, max_bits, None, 0)
+    out = np.zeros(max(n, 1), dtype=np.uint64)
+    lib().cave_enumerate_valid_bitmasks(neighbor_count, max_bits, _u64p(out), n)
+    return out[:n].copy()
+
+
+class Context:
+    """One device + stream (cave_ctx)."""
+
+    def __init__(self, device=0):
+        h = ctypes.c_void_p()
+        rc = lib().cave_ctx_create(device, ctypes.byref(h))
+        if rc != OK:
+            raise CaveError(rc, f"cave_ctx_create({device}) failed: {lib().cave_status_string(rc).decode()}")
+        self.h = h
+
+    def check(self, rc, what):
+        if rc != OK:
+            raise CaveError(rc, f"{what}: {lib().cave_status_string(rc).decode()}: "
+                                f"{lib().cave_last_error(self.h).decode()}")
+
+    def synchronize(self):
+        self.check(lib().cave_ctx_synchronize(self.h), "cave_ctx_synchronize")
+
+    def close(self):
+        if self.h:
+            lib().cave_ctx_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+class Grid:
+    """A device grid in the reference's padded nibble layout (cave_grid)."""
+
+    def __init__(self, ctx: Context, X, Y, Z):
+        self.ctx, self.X, self.Y, self.Z = ctx, X, Y, Z
+        h = ctypes.c_void_p()
+        ctx.check(lib().cave_grid_create(ctx.h, X, Y, Z, ctypes.byref(h)), "cave_grid_create")
+        self.h = h
+        self.words = grid_words(X, Y, Z)
+
+    def close(self):
+        if self.h:
+            lib().cave_grid_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def upload(self, words):
+        w = np.ascontiguousarray(words, dtype=np.uint32)
+        self.ctx.check(lib().cave_grid_upload(self.h, _u32p(w), w.size), "cave_grid_upload")
+
+    def download(self) -> np.ndarray:
+        out = np.zeros(self.words, dtype=np.uint32)
+        self.ctx.check(lib().cave_grid_download(self.h, _u32p(out), out.size), "cave_grid_download")
+        return out
+
+    def seed(self, chunk: ChunkConfig, max_cell_state):
+        self.ctx.check(lib().cave_grid_seed(self.h, ctypes.byref(chunk), max_cell_state), "cave_grid_seed")
+
+    def seed_threshold(self, spawn, threshold, run_seed, max_cell_state):
+        self.ctx.check(lib().cave_grid_seed_threshold(self.h, spawn[0], spawn[1], spawn[2], threshold, run_seed,
+                                                      max_cell_state), "cave_grid_seed_threshold")
+
+    def step(self, params: SimParams, nticks=1, valid=None, max_rule_bits=0, stats=True):
+        """Plain path (one launch per tick). Returns the list of per-tick TickStats."""
+        v = None if valid is None else np.ascontiguousarray(valid, dtype=np.uint64)
+        pt = (TickStats * max(nticks, 1))() if stats else None
+        self.ctx.check(lib().cave_step(self.h, ctypes.byref(params), _u64p(v), 0 if v is None else v.size,
+                                       max_rule_bits, nticks, pt), "cave_step")
+        return [pt[i] for i in range(nticks)] if stats else None
+
+    def run(self, params: SimParams, nticks, max_ticks=None, valid=None, max_rule_bits=0, stats=True):
+        """Streaming path. Returns (per-tick TickStats list, GridInfo)."""
+        v = None if valid is None else np.ascontiguousarray(valid, dtype=np.uint64)
+        pt = (TickStats * max(nticks, 1))() if stats else None
+        info = GridInfo()
+        self.ctx.check(lib().cave_run(self.h, ctypes.byref(params), _u64p(v), 0 if v is None else v.size,
+                                      max_rule_bits, nticks, nticks if max_ticks is None else max_ticks, pt,
+                                      ctypes.byref(info)), "cave_run")
+        return ([pt[i] for i in range(nticks)] if stats else None), info
+
+
+def manager_update(snapshot: GridSnapshot, info: GridInfo, perms: SimParams, max_permutation, survival_end,
+                   max_ticks):
+    ic, pc = GridInfo(), SimParams()
+    lib().cave_manager_update(ctypes.byref(snapshot), ctypes.byref(info), ctypes.byref(perms), max_permutation,
+                              survival_end, max_ticks, ctypes.byref(ic), ctypes.byref(pc))
+    return ic, pc

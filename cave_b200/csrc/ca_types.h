@@ -1,0 +1,57 @@
+// ca_types.h -- rule and geometry types shared by host code and the sm_100a kernels.
+#pragma once
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define CAVE_HD __host__ __device__
+#else
+#define CAVE_HD
+#endif
+
+namespace cave {
+
+// One count value k that appears in the survival or birth table (sparse rule evaluation).
+struct RuleTerm {
+    uint32_t nk[5];    // nk[i] = ~0 if bit i of k is 0 else 0 (so (c_i ^ nk_i) is 1 where c_i == k_i)
+    uint32_t sm, bm;   // ~0 if k is in lut_s / lut_b
+    uint32_t pad;
+};
+static_assert(sizeof(RuleTerm) == 32, "RuleTerm is two 16-byte words");
+
+constexpr int kMaxTerms = 8;  // the sparse path handles rules with <= kMaxTerms distinct counts
+
+// Decoded rule for one simulation, in the form the kernels consume.
+//   lut_s: bit b set  <=> an alive cell whose row-sum count is b survives
+//   lut_b: bit b set  <=> a dead cell whose count is b is born
+// (the reference's survival/birth masks shifted by 1, plus 1 more for an alive cell when
+//  the neighbourhood contains faces, because the row sums then include the cell itself).
+struct DeviceRule {
+    uint32_t maxcs;        // 1..16 (16 = the encoded value 15: nothing is ever alive)
+    uint32_t flags;        // neighbourhood bits F=1 E=2 C=4 (wrap bit 8 is ignored by the cube shader)
+    uint32_t lut_s, lut_b;
+    uint32_t m[4];         // m[i] = ~0 if bit i of maxcs is set (maxcs & 15)
+    uint32_t alive_ok;     // ~0 unless maxcs == 16
+    uint32_t nterms;       // number of entries in terms[] (0 => use the LUT tree)
+    uint32_t pad[2];
+    RuleTerm terms[kMaxTerms];
+};
+
+// Count planes needed per neighbourhood (max count: F 7, E 12, FE 19, C 8, FC 15, EC 20,
+// FEC 27, where the F-containing ones include the cell itself); nb = 0 counts nothing.
+CAVE_HD constexpr int count_bits(int nb) {
+    return nb == 0 ? 1 : nb == 1 ? 3 : (nb == 2 || nb == 4 || nb == 5) ? 4 : 5;
+}
+CAVE_HD constexpr bool counts_self(int nb) { return (nb & 1) != 0; }
+CAVE_HD constexpr int max_count(int nb) {
+    return nb == 0 ? 0 : nb == 1 ? 7 : nb == 2 ? 12 : nb == 3 ? 19 : nb == 4 ? 8 : nb == 5 ? 15 : nb == 6 ? 20 : 27;
+}
+
+// Valid-cell mask of strip sx in a row of X cells.
+CAVE_HD inline uint32_t strip_valid(uint32_t sx, uint32_t X) {
+    const uint32_t x0 = sx * 32u;
+    if (x0 >= X) return 0u;
+    const uint32_t n = X - x0;
+    return n >= 32u ? 0xFFFFFFFFu : ((1u << n) - 1u);
+}
+
+}  // namespace cave

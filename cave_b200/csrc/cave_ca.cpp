@@ -1,0 +1,384 @@
+// cave_ca.cpp -- C ABI of libcave_ca.so: contexts, grids, the plain path, the streaming path.
+#include "../../include/cave_ca.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "context.h"
+#include "kernels.h"
+#include "rules.h"
+
+namespace cave {
+
+cave_status set_error(cave_ctx* ctx, cave_status code, const std::string& msg) {
+    if (ctx) {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        ctx->last_error = msg;
+    }
+    return code;
+}
+
+cave_status check_cuda(cave_ctx* ctx, cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return CAVE_OK;
+    const cave_status code = (e == cudaErrorMemoryAllocation) ? CAVE_ERR_OUT_OF_MEMORY : CAVE_ERR_CUDA;
+    return set_error(ctx, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+static uint32_t resolve_spawn(uint32_t axis, uint32_t sizeIndex) {  // searchSystem.cpp:226-232
+    if (sizeIndex == 0) return axis;
+    uint32_t scaled = (uint32_t)(((uint64_t)axis * (sizeIndex + 1) + 15) / 16);
+    return std::max(1u, std::min(axis, scaled));
+}
+
+SeedSpec make_seed_spec(uint32_t X, uint32_t Y, uint32_t Z, uint32_t sx, uint32_t sy, uint32_t sz,
+                        uint32_t spawnSizeIndex, uint64_t threshold, bool fill_all, uint32_t seed,
+                        uint32_t maxcs) {
+    SeedSpec sp;
+    sp.X = X;
+    sp.Y = Y;
+    sp.Z = Z;
+    const uint32_t dims[3] = {X, Y, Z};
+    const uint32_t sp_in[3] = {std::min(sx, X), std::min(sy, Y), std::min(sz, Z)};
+    for (int k = 0; k < 3; k++) {
+        const uint32_t e = resolve_spawn(sp_in[k], spawnSizeIndex);
+        sp.lo[k] = (dims[k] - e) / 2;  // searchSystem.cpp:270-273
+        sp.hi[k] = (dims[k] + e) / 2;
+    }
+    sp.threshold = threshold;
+    sp.fill_all = fill_all ? 1u : 0u;
+    sp.seed = seed;
+    sp.maxcs = maxcs;
+    return sp;
+}
+
+bool plan_stream(uint32_t sim_index, uint32_t X, uint32_t Y, uint32_t Z, uint32_t target_ctas, uint32_t rows_hint,
+                 StreamPlan& plan) {
+    const uint32_t SX = (X + 31u) / 32u;
+    if (SX == 0 || SX > 32 || Y == 0 || Z == 0 || Y > 65535 || Z > 65535) return false;
+    uint32_t SXp = 1;
+    while (SXp < SX) SXp <<= 1;
+    const uint32_t step = std::max(1u, 32u / SXp);  // rows must keep threads a multiple of 32
+    uint32_t rows = rows_hint ? rows_hint : std::max(512u / SXp, 3u);
+    rows = std::min(rows, 1024u / SXp);
+    rows = std::min(rows, Y + 2u);
+    rows = (rows + step - 1) / step * step;
+    if (rows < 3) rows = 3 * step;
+    const uint32_t TY = rows - 2;
+    const uint32_t ny = (Y + TY - 1) / TY;
+    const uint32_t ty = (Y + ny - 1) / ny;
+    uint32_t nz = std::max(1u, target_ctas / ny);
+    nz = std::min(nz, Z);
+    const uint32_t slab = (Z + nz - 1) / nz;
+    nz = (Z + slab - 1) / slab;
+    plan.SX = SX;
+    plan.SXp = SXp;
+    plan.rows = rows;
+    plan.threads = rows * SXp;
+    plan.ny = ny;
+    plan.nz = nz;
+    plan.items.clear();
+    for (uint32_t iz = 0; iz < nz; iz++) {
+        for (uint32_t iy = 0; iy < ny; iy++) {
+            StreamItem it;
+            it.sim = sim_index;
+            it.y0 = (uint16_t)(iy * ty);
+            it.ty = (uint16_t)std::min(ty, Y - iy * ty);
+            it.z0 = (uint16_t)(iz * slab);
+            it.z1 = (uint16_t)std::min(Z, (iz + 1) * slab);
+            it.dir = iz & 1u;
+            plan.items.push_back(it);
+        }
+    }
+    return true;
+}
+
+}  // namespace cave
+
+using namespace cave;
+
+extern "C" {
+
+const char* cave_status_string(cave_status s) {
+    switch (s) {
+        case CAVE_OK: return "ok";
+        case CAVE_ERR_INVALID_ARG: return "invalid argument";
+        case CAVE_ERR_CUDA: return "CUDA error";
+        case CAVE_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case CAVE_ERR_NOT_READY: return "not ready";
+        case CAVE_ERR_TIMEOUT: return "device-side wait timed out";
+        case CAVE_ERR_IO: return "I/O error";
+        case CAVE_ERR_INTERNAL: return "internal error";
+        default: return "unknown status";
+    }
+}
+
+const char* cave_last_error(const cave_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "no context"; }
+
+cave_status cave_ctx_create(int device, cave_ctx** out) {
+    if (!out) return CAVE_ERR_INVALID_ARG;
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || device < 0 || device >= n) return CAVE_ERR_CUDA;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return CAVE_ERR_CUDA;
+    if (prop.major != 10) return CAVE_ERR_CUDA;  // the kernels are built for sm_100a only
+    cave_ctx* c = new (std::nothrow) cave_ctx();
+    if (!c) return CAVE_ERR_OUT_OF_MEMORY;
+    c->device = device;
+    c->sm_count = prop.multiProcessorCount;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return CAVE_ERR_CUDA;
+    }
+    *out = c;
+    return CAVE_OK;
+}
+
+void cave_ctx_destroy(cave_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaStreamDestroy(ctx->stream);
+    }
+    delete ctx;
+}
+
+cave_status cave_ctx_synchronize(cave_ctx* ctx) {
+    if (!ctx) return CAVE_ERR_INVALID_ARG;
+    CAVE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return CAVE_OK;
+}
+
+uint64_t cave_grid_words(uint32_t X, uint32_t Y, uint32_t Z) { return (uint64_t)((X + 7u) / 8u) * Y * Z; }
+
+static cave::PlainSlot fresh_slot() {
+    cave::PlainSlot s;
+    std::memset(&s, 0, sizeof(s));
+    for (int k = 0; k < 3; k++) {
+        s.bmin[k] = 0xFFFFFFFFu;
+        s.bmax[k] = 0;
+    }
+    return s;
+}
+
+cave_status cave_grid_create(cave_ctx* ctx, uint32_t X, uint32_t Y, uint32_t Z, cave_grid** out) {
+    if (!ctx || !out) return CAVE_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (X == 0 || Y == 0 || Z == 0 || (uint64_t)X * Y * Z >= (1ull << 32))
+        return set_error(ctx, CAVE_ERR_INVALID_ARG, "grid volume must be in [1, 2^32)");
+    CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
+    cave_grid* g = new (std::nothrow) cave_grid();
+    if (!g) return CAVE_ERR_OUT_OF_MEMORY;
+    g->ctx = ctx;
+    g->X = X;
+    g->Y = Y;
+    g->Z = Z;
+    g->words = cave_grid_words(X, Y, Z);
+    cudaError_t e = cudaMalloc(&g->nib[0], g->words * 4 * 2);
+    if (e == cudaSuccess) {
+        g->nib[1] = g->nib[0] + g->words;
+        e = cudaMalloc(&g->slot, sizeof(cave::PlainSlot));
+    }
+    if (e == cudaSuccess) e = cudaMemsetAsync(g->nib[0], 0, g->words * 4 * 2, ctx->stream);
+    if (e == cudaSuccess) {
+        cave::PlainSlot s = fresh_slot();
+        e = cudaMemcpyAsync(g->slot, &s, sizeof(s), cudaMemcpyHostToDevice, ctx->stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        cudaFree(g->nib[0]);
+        cudaFree(g->slot);
+        delete g;
+        return check_cuda(ctx, e, "cave_grid_create");
+    }
+    *out = g;
+    return CAVE_OK;
+}
+
+void cave_grid_destroy(cave_grid* g) {
+    if (!g) return;
+    cudaSetDevice(g->ctx->device);
+    cudaStreamSynchronize(g->ctx->stream);
+    cudaFree(g->nib[0]);
+    cudaFree(g->slot);
+    cudaFree(g->strips);
+    cudaFree(g->sim);
+    delete g;
+}
+
+cave_status cave_grid_upload(cave_grid* g, const uint32_t* words, uint64_t nwords) {
+    if (!g || !words || nwords != g->words) return CAVE_ERR_INVALID_ARG;
+    cave_ctx* ctx = g->ctx;
+    CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
+    CAVE_CUDA(ctx, cudaMemcpyAsync(g->nib[g->cur], words, nwords * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CAVE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return CAVE_OK;
+}
+
+cave_status cave_grid_download(cave_grid* g, uint32_t* words, uint64_t nwords) {
+    if (!g || !words || nwords != g->words) return CAVE_ERR_INVALID_ARG;
+    cave_ctx* ctx = g->ctx;
+    CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
+    CAVE_CUDA(ctx, cudaMemcpyAsync(words, g->nib[g->cur], nwords * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CAVE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return CAVE_OK;
+}
+
+static cave_status seed_grid(cave_grid* g, const SeedSpec& sp) {
+    cave_ctx* ctx = g->ctx;
+    CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
+    CAVE_CUDA(ctx, launch_seed_nib(g->nib[g->cur], sp, ctx->stream));
+    CAVE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return CAVE_OK;
+}
+
+cave_status cave_grid_seed(cave_grid* g, const cave_chunk_config* c, uint32_t maxCellState) {
+    if (!g || !c || c->spawnDensityIndex > 15) return CAVE_ERR_INVALID_ARG;
+    if (c->gridDimensionX != g->X || c->gridDimensionY != g->Y || c->gridDimensionZ != g->Z)
+        return set_error(g->ctx, CAVE_ERR_INVALID_ARG, "chunk grid dimensions differ from the grid's");
+    const bool random = c->spawnRegionShapeId == 0;  // searchSystem.cpp:238
+    const float density = ((float)c->spawnDensityIndex + 1.0f) / 16.0f;  // :240
+    const bool all = !random || density >= 1.0f;
+    const uint64_t thr = all ? (1ull << 32) : (uint64_t)(uint32_t)(density * 4294967296.0);  // :260-262
+    SeedSpec sp = make_seed_spec(g->X, g->Y, g->Z, c->spawnAreaDimensionX, c->spawnAreaDimensionY,
+                                 c->spawnAreaDimensionZ, c->spawnSizeIndex, thr, all, c->runSeedIndex, maxCellState);
+    return seed_grid(g, sp);
+}
+
+cave_status cave_grid_seed_threshold(cave_grid* g, uint32_t spawnX, uint32_t spawnY, uint32_t spawnZ,
+                                     uint64_t threshold, uint32_t runSeedIndex, uint32_t maxCellState) {
+    if (!g || threshold > (1ull << 32)) return CAVE_ERR_INVALID_ARG;
+    SeedSpec sp = make_seed_spec(g->X, g->Y, g->Z, spawnX, spawnY, spawnZ, 0, threshold, threshold == (1ull << 32),
+                                 runSeedIndex, maxCellState);
+    return seed_grid(g, sp);
+}
+
+// Device copy of the K-index table (nullptr when not used).
+struct DevTable {
+    uint64_t* p = nullptr;
+    ~DevTable() { cudaFree(p); }
+};
+
+cave_status cave_step(cave_grid* g, const cave_sim_params* params, const uint64_t* validBitmasks, uint32_t nValid,
+                      uint32_t maxRuleBits, uint32_t nticks, cave_tick_stats* per_tick) {
+    if (!g || !params) return CAVE_ERR_INVALID_ARG;
+    cave_ctx* ctx = g->ctx;
+    DecodedRule d;
+    if (!decode_params(*params, validBitmasks, nValid, maxRuleBits, d))
+        return set_error(ctx, CAVE_ERR_INVALID_ARG, "rule index outside the valid-bitmask table");
+    if (nticks == 0) return CAVE_OK;
+    CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
+    DevTable tab;
+    if (maxRuleBits > 0) {
+        CAVE_CUDA(ctx, cudaMalloc(&tab.p, sizeof(uint64_t) * nValid));
+        CAVE_CUDA(ctx, cudaMemcpyAsync(tab.p, validBitmasks, sizeof(uint64_t) * nValid, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    cave_tick_stats* dticks = nullptr;
+    if (per_tick) CAVE_CUDA(ctx, cudaMalloc(&dticks, sizeof(cave_tick_stats) * nticks));
+    PlainSlot s = fresh_slot();
+    s.perms = *params;
+    s.run_manager = 0;
+    s.per_tick = dticks;
+    cudaError_t e = cudaMemcpyAsync(g->slot, &s, sizeof(s), cudaMemcpyHostToDevice, ctx->stream);
+    for (uint32_t t = 0; t < nticks && e == cudaSuccess; t++) {
+        e = launch_plain_step(g->nib[g->cur], g->nib[g->cur ^ 1], g->X, g->Y, g->Z, g->slot, tab.p, nValid,
+                              maxRuleBits, ctx->stream);
+        g->cur ^= 1;
+    }
+    if (e == cudaSuccess && per_tick)
+        e = cudaMemcpyAsync(per_tick, dticks, sizeof(cave_tick_stats) * nticks, cudaMemcpyDeviceToHost, ctx->stream);
+    PlainSlot back;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&back, g->slot, sizeof(back), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(dticks);
+    if (e != cudaSuccess) return check_cuda(ctx, e, "cave_step");
+    if (back.error) return set_error(ctx, CAVE_ERR_INTERNAL, "plain kernel raised an error flag");
+    return CAVE_OK;
+}
+
+cave_status cave_run(cave_grid* g, const cave_sim_params* params, const uint64_t* validBitmasks, uint32_t nValid,
+                     uint32_t maxRuleBits, uint32_t nticks, uint32_t maxTicks, cave_tick_stats* per_tick,
+                     cave_grid_info* info) {
+    if (!g || !params) return CAVE_ERR_INVALID_ARG;
+    cave_ctx* ctx = g->ctx;
+    DecodedRule d;
+    if (!decode_params(*params, validBitmasks, nValid, maxRuleBits, d))
+        return set_error(ctx, CAVE_ERR_INVALID_ARG, "rule index outside the valid-bitmask table");
+    StreamPlan plan;
+    if (!plan_stream(0, g->X, g->Y, g->Z, (uint32_t)ctx->sm_count * 2, 0, plan))
+        return set_error(ctx, CAVE_ERR_INVALID_ARG, "grid shape not supported by the streaming kernel (X <= 1024, Y,Z <= 65535)");
+    CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
+    const uint64_t nstrips = (uint64_t)plan.SX * g->Y * g->Z;
+    if (!g->strips) {
+        CAVE_CUDA(ctx, cudaMalloc(&g->strips, nstrips * 16 * 2));
+        CAVE_CUDA(ctx, cudaMalloc(&g->sim, sizeof(StripSim)));
+        g->strip_count = nstrips;
+    }
+    StripSim s;
+    std::memset(&s, 0, sizeof(s));
+    s.rule = make_device_rule(d);
+    s.X = g->X;
+    s.Y = g->Y;
+    s.Z = g->Z;
+    s.SX = plan.SX;
+    s.buf[0] = 0;
+    s.buf[1] = nstrips * 16;
+    s.max_ticks = maxTicks;
+    s.tick_limit = nticks;
+    s.stop_on_status = 0;
+    s.n_items = (uint32_t)plan.items.size();
+    for (int k = 0; k < 3; k++) s.acc_bmin[k] = 0xFFFFFFFFu;
+    cave_tick_stats* dticks = nullptr;
+    StreamItem* ditems = nullptr;
+    if (per_tick && nticks) CAVE_CUDA(ctx, cudaMalloc(&dticks, sizeof(cave_tick_stats) * nticks));
+    s.per_tick = dticks;
+    cudaError_t e = cudaMalloc(&ditems, sizeof(StreamItem) * plan.items.size());
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(ditems, plan.items.data(), sizeof(StreamItem) * plan.items.size(), cudaMemcpyHostToDevice,
+                            ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(g->sim, &s, sizeof(s), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = launch_nib_to_strips(g->nib[g->cur], g->strips, g->X, g->Y, g->Z, ctx->stream);
+    const bool sparse = rule_is_sparse(s.rule);
+    for (uint32_t t = 0; t < nticks && e == cudaSuccess; t++)
+        e = launch_stream_tick((int)(d.flags & 7u), sparse, ditems, (uint32_t)plan.items.size(), g->sim, g->strips,
+                               plan.SX, plan.SXp, plan.threads, ctx->stream);
+    StripSim back;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&back, g->sim, sizeof(back), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) {
+        const uint4* cur = g->strips + (back.tick & 1u) * nstrips;
+        e = launch_strips_to_nib(cur, g->nib[g->cur], g->X, g->Y, g->Z, ctx->stream);
+    }
+    if (e == cudaSuccess && per_tick && nticks)
+        e = cudaMemcpyAsync(per_tick, dticks, sizeof(cave_tick_stats) * nticks, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(dticks);
+    cudaFree(ditems);
+    if (e != cudaSuccess) return check_cuda(ctx, e, "cave_run");
+    if (back.error & kErrWaitTimeout) return set_error(ctx, CAVE_ERR_TIMEOUT, "streaming kernel: bulk-copy wait timed out");
+    if (back.error) return set_error(ctx, CAVE_ERR_INTERNAL, "streaming kernel raised an error flag");
+    if (info) *info = back.info;
+    return CAVE_OK;
+}
+
+void cave_manager_update(const cave_grid_snapshot* snapshot, cave_grid_info* info, cave_sim_params* perms,
+                         uint64_t maxPermutation, uint64_t survivalEndPermutation, uint32_t maxTicks,
+                         cave_grid_info* infoCopy, cave_sim_params* permsCopy) {
+    if (!snapshot || !info || !perms || !infoCopy || !permsCopy) return;
+    manager_update(*snapshot, *info, *perms, maxPermutation, survivalEndPermutation, maxTicks, *infoCopy, *permsCopy);
+}
+
+uint64_t cave_enumerate_valid_bitmasks(uint32_t neighborCount, uint32_t maxBits, uint64_t* out, uint64_t cap) {
+    std::vector<uint64_t> v = enumerate_valid_bitmasks(neighborCount, maxBits);
+    if (out) std::memcpy(out, v.data(), sizeof(uint64_t) * std::min<uint64_t>(cap, v.size()));
+    return v.size();
+}
+
+}  // extern "C"

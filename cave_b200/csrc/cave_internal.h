@@ -1,0 +1,110 @@
+// cave_internal.h -- device-side records shared by the kernels and the host library.
+#pragma once
+#include <cstdint>
+
+#include "../../include/cave_ca.h"
+#include "ca_types.h"
+#include <vector_types.h>
+
+namespace cave {
+
+constexpr uint64_t kPermMask = (uint64_t(1) << 60) - 1;  // simulation.h:43
+
+// Bounded device-side waits give up after this many polls and raise an error flag.
+constexpr uint32_t kSpinLimit = 1u << 26;
+
+// Error flags a kernel may raise in its record (read back by the host).
+enum : uint32_t { kErrNone = 0, kErrWaitTimeout = 1, kErrBadRuleIndex = 2 };
+
+// Per-grid device record of the plain path. It holds what the reference keeps in the
+// per-slot permutation / snapshot / GridInfo / copy buffers (searchSystem.cpp:202-374).
+struct PlainSlot {
+    cave_sim_params perms;        // gridPermutationsBuffer (live; the manager advances it)
+    uint32_t run_manager;         // 1: apply searchManager semantics after each tick
+    uint32_t error;               // kErr* flags
+    // tick accumulators (zeroed again by the last CTA of each tick)
+    uint32_t acc[4];              // dead, dying, born, surviving (GridSnapshot order)
+    uint32_t population;
+    uint32_t bmin[3], bmax[3];
+    uint32_t ticket;
+    cave_grid_info info;          // gridInfoBuffer
+    cave_grid_info infoCopy;      // gridInfoCopyBuffer
+    cave_sim_params permsCopy;    // gridPermutationsCopyBuffer
+    uint64_t maxPermutation;      // gridMaxPermutationBuffer
+    uint64_t survivalEnd;         // gridSurvivalEndPermutationBuffer
+    uint32_t maxTicks;            // MAX_NUMBER_OF_TICKS_TO_SURVIVE
+    uint32_t tick_count;          // ticks folded since the slot was reset
+    cave_tick_stats last;         // statistics of the most recent tick
+    cave_tick_stats* per_tick;    // optional device array indexed by tick_count
+};
+
+// Host+device restatement of searchManager.slang:56-149 on plain structs.
+CAVE_HD inline void manager_update(const cave_grid_snapshot& snap, cave_grid_info& info,
+                                               cave_sim_params& perms, uint64_t maxPermutation,
+                                               uint64_t survivalEnd, uint32_t maxTicks, cave_grid_info& infoCopy,
+                                               cave_sim_params& permsCopy) {
+    cave_sim_params p = perms;
+    if (p.survivalAndNeighborhoodRules == 0 || p.birthAndMaxCellStateRules == 0) {
+        infoCopy = info;
+        permsCopy = p;
+        return;
+    }
+    info.numberOfSimulationTicksSurvived++;
+    info.totalNumberOfCellsThatDied += snap.numberOfDeadCells;
+    info.totalNumberOfCellsThatWereBorn += snap.numberOfCellsBorn;
+    info.finalAliveCount = snap.numberOfSurvivingCells;
+    if (snap.numberOfSurvivingCells > info.maxAliveCount) info.maxAliveCount = snap.numberOfSurvivingCells;
+    if (snap.numberOfSurvivingCells == 0u && snap.numberOfCellsBorn == 0u)
+        info.status = 1;
+    else if (info.numberOfSimulationTicksSurvived >= maxTicks)
+        info.status = 2;
+    else
+        info.status = 0;
+    infoCopy = info;
+    permsCopy = p;
+    if (info.status > 0) {
+        // NextPermutation (searchManager.slang:56-96)
+        if ((p.birthAndMaxCellStateRules & kPermMask) < maxPermutation) {
+            p.birthAndMaxCellStateRules++;
+        } else if ((p.survivalAndNeighborhoodRules & kPermMask) < survivalEnd) {
+            p.survivalAndNeighborhoodRules++;
+            p.birthAndMaxCellStateRules = (p.birthAndMaxCellStateRules & ~kPermMask) + 1;
+        } else {
+            p.survivalAndNeighborhoodRules = 0;
+            p.birthAndMaxCellStateRules = 0;
+            perms = p;
+            return;
+        }
+        perms = p;
+        info = cave_grid_info{0, 0, 0, 0, 0, 0};
+    }
+}
+
+// ---- bit-plane (strip) path -----------------------------------------------------------
+// Per-simulation device record of the strip kernels.
+struct StripSim {
+    DeviceRule rule;
+    uint32_t X, Y, Z, SX;       // SX = strips per row
+    uint64_t buf[2];            // byte offsets (into the strip pool) of the two cell copies
+    uint32_t max_ticks;         // MAX_NUMBER_OF_TICKS_TO_SURVIVE
+    uint32_t tick_limit;        // ticks to run in total (raw stepping) or max_ticks (search)
+    uint32_t stop_on_status;    // 1: stop when the manager reports status > 0
+    uint32_t n_items;           // CTAs (work items) per tick for this simulation
+    uint32_t tick;              // ticks completed
+    uint32_t done;              // no further ticks run
+    uint32_t error;
+    uint32_t ticket;
+    cave_grid_info info;        // manager state (searchManager.slang GridInfo semantics)
+    // per-tick accumulators
+    uint32_t acc_surv, acc_born, acc_zero, acc_pop;
+    uint32_t acc_bmin[3], acc_bmax[3];
+    // derived totals
+    uint32_t prev_pop;
+    uint32_t pop_change_ticks;
+    uint64_t total_changed;
+    cave_tick_stats last;
+    cave_tick_stats* per_tick;  // optional, tick_limit entries
+    uint64_t pad;
+};
+
+}  // namespace cave

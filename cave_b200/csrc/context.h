@@ -1,0 +1,62 @@
+// context.h -- host-side objects behind the opaque handles of cave_ca.h.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "cave_internal.h"
+#include "kernels.h"
+
+struct cave_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int sm_count = 148;
+    std::string last_error;
+    std::mutex mu;  // guards last_error
+};
+
+struct cave_grid {
+    cave_ctx* ctx = nullptr;
+    uint32_t X = 0, Y = 0, Z = 0;
+    uint64_t words = 0;
+    uint32_t* nib[2] = {nullptr, nullptr};  // ping-pong nibble copies
+    int cur = 0;                             // index of the current copy
+    cave::PlainSlot* slot = nullptr;         // plain-path record
+    // strip path (allocated on first cave_run)
+    uint4* strips = nullptr;                 // 2 copies back to back
+    uint64_t strip_count = 0;                // strips per copy
+    cave::StripSim* sim = nullptr;
+};
+
+namespace cave {
+
+// Records `msg` as the context's last error and returns `code`.
+cave_status set_error(cave_ctx* ctx, cave_status code, const std::string& msg);
+// Checks a CUDA call; on failure records the error text.
+cave_status check_cuda(cave_ctx* ctx, cudaError_t e, const char* what);
+
+#define CAVE_CUDA(ctx, call)                                         \
+    do {                                                             \
+        cudaError_t _e = (call);                                     \
+        if (_e != cudaSuccess) return ::cave::check_cuda(ctx, _e, #call); \
+    } while (0)
+
+// Tiling of one simulation for the streaming tick kernel.
+struct StreamPlan {
+    uint32_t SX, SXp, threads, rows;
+    uint32_t ny, nz;       // y-tiles and z-slabs
+    std::vector<StreamItem> items;
+};
+// Builds the work items of simulation `sim_index` with grid X*Y*Z; `target_ctas` is the
+// number of CTAs one tick should spread over (a multiple of the SM count).
+bool plan_stream(uint32_t sim_index, uint32_t X, uint32_t Y, uint32_t Z, uint32_t target_ctas,
+                 uint32_t rows_hint, StreamPlan& plan);
+
+SeedSpec make_seed_spec(uint32_t X, uint32_t Y, uint32_t Z, uint32_t sx, uint32_t sy, uint32_t sz,
+                        uint32_t spawnSizeIndex, uint64_t threshold, bool fill_all, uint32_t seed,
+                        uint32_t maxcs);
+
+}  // namespace cave

@@ -1,0 +1,43 @@
+// kernels.h -- launch entry points of the CUDA kernels (host-callable, C++ linkage).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "cave_internal.h"
+
+namespace cave {
+
+// Spawn box and fill of searchSystem.cpp:219-306, resolved on the host.
+struct SeedSpec {
+    uint32_t X, Y, Z;
+    uint32_t lo[3], hi[3];   // box [lo, hi) per axis
+    uint64_t threshold;      // alive iff cellHash < threshold
+    uint32_t fill_all;       // density >= 1 (or filled spawn): every box cell alive
+    uint32_t seed;           // runSeedIndex
+    uint32_t maxcs;          // written as (maxcs & 0xF)
+};
+
+// One CTA's share of one tick of one simulation in the streaming kernel.
+struct StreamItem {
+    uint32_t sim;            // index into the StripSim array
+    uint16_t y0, ty;         // output rows [y0, y0 + ty)
+    uint16_t z0, z1;         // output planes [z0, z1)
+    uint32_t dir;            // 0: march towards +z, 1: towards -z
+};
+
+cudaError_t launch_plain_step(const uint32_t* in, uint32_t* out, uint32_t X, uint32_t Y, uint32_t Z,
+                              PlainSlot* slot, const uint64_t* valid, uint32_t nValid, uint32_t maxRuleBits,
+                              cudaStream_t stream);
+cudaError_t launch_nib_to_strips(const uint32_t* nib, uint4* strips, uint32_t X, uint32_t Y, uint32_t Z,
+                                 cudaStream_t st);
+cudaError_t launch_strips_to_nib(const uint4* strips, uint32_t* nib, uint32_t X, uint32_t Y, uint32_t Z,
+                                 cudaStream_t st);
+cudaError_t launch_seed_nib(uint32_t* nib, const SeedSpec& sp, cudaStream_t st);
+cudaError_t launch_seed_strips(uint4* strips, const SeedSpec& sp, cudaStream_t st);
+// threads = rows * SXp (rows includes the two halo rows), SXp = power of two >= SX, <= 32.
+cudaError_t launch_stream_tick(int nb, bool sparse, const StreamItem* items, uint32_t n_items, StripSim* sims,
+                               uint4* pool, uint32_t SX, uint32_t SXp, uint32_t threads, cudaStream_t st);
+size_t stream_smem_bytes_host(uint32_t rows, uint32_t SX, uint32_t SXp);
+
+}  // namespace cave

@@ -1,0 +1,167 @@
+/*
+ * cave_ca.h -- C ABI of the B200 (sm_100a) CA stepping library (libcave_ca.so).
+ *
+ * Drop-in for the search-mode stepping path of CAVE (Scub3d/CAVE). The reference has no
+ * FFI of its own: its hot path sits behind a Vulkan shader-binding contract and the C++
+ * class SearchSystem. Each entry point below names the reference interface it replaces.
+ *
+ * Conventions: every function returns cave_status (0 = CAVE_OK); no C++ exception crosses
+ * this boundary; host buffers are caller-owned; device buffers are library-owned and
+ * addressed by opaque handles; one CUDA stream per context; a context may be used from one
+ * host thread at a time. cave_last_error() returns the context's last error text.
+ *
+ * Cell layout at this boundary is the reference's padded nibble layout
+ * (searchSimulationCube.slang:52-53, :88-93; searchSystem.cpp:140-143, :290-295):
+ * 4 bits per cell, 8 cells per uint32 along x (low nibble = lowest x), word index
+ * x/8 + y*W + z*W*Y with W = ceil(X/8); padding nibbles are 0.
+ */
+#ifndef CAVE_CA_H
+#define CAVE_CA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int cave_status;
+enum {
+    CAVE_OK = 0,
+    CAVE_ERR_INVALID_ARG = 1,   /* bad size, pointer, rule index, or unsupported geometry */
+    CAVE_ERR_CUDA = 2,          /* a CUDA runtime call failed (text in cave_last_error)   */
+    CAVE_ERR_OUT_OF_MEMORY = 3, /* device allocation or admission budget exceeded          */
+    CAVE_ERR_NOT_READY = 4,     /* non-blocking poll: work still in flight                 */
+    CAVE_ERR_TIMEOUT = 5,       /* a bounded device-side wait gave up (kernel error flag) */
+    CAVE_ERR_IO = 6,            /* JSONL output could not be written                       */
+    CAVE_ERR_INTERNAL = 7
+};
+
+/* ---- reference data structures (bit-exact layouts) --------------------------------- */
+
+/* SimulationParameters (src/common/structs.h:89-99; encoding simulation.h:43-59):
+ *   birthAndMaxCellStateRules    [63:60] = maxCellState-1, [59:0] birth mask or 1-based K-index
+ *   survivalAndNeighborhoodRules [63:60] = flags W=8 C=4 E=2 F=1, [59:0] survival mask or K-index
+ *   shapeAndGridConfiguration    [4:0] shape id (0 = cube)                                 */
+typedef struct {
+    uint64_t birthAndMaxCellStateRules;
+    uint64_t survivalAndNeighborhoodRules;
+    uint64_t shapeAndGridConfiguration;
+} cave_sim_params;
+
+/* GridSnapshot (structs.h:130-136). */
+typedef struct {
+    uint32_t numberOfDeadCells;
+    uint32_t numberOfDyingCells;
+    uint32_t numberOfCellsBorn;
+    uint32_t numberOfSurvivingCells;
+} cave_grid_snapshot;
+
+/* GridInfo (structs.h:79-87). */
+typedef struct {
+    uint32_t totalNumberOfCellsThatDied;
+    uint32_t totalNumberOfCellsThatWereBorn;
+    uint32_t numberOfSimulationTicksSurvived;
+    uint32_t status; /* 0 running, 1 early death, 2 reached the tick limit (viable) */
+    uint32_t maxAliveCount;
+    uint32_t finalAliveCount;
+} cave_grid_info;
+
+/* ChunkConfiguration (structs.h:109-128). */
+typedef struct {
+    uint32_t shapeId;
+    uint32_t gridDimensionX, gridDimensionY, gridDimensionZ;
+    uint32_t spawnAreaDimensionX, spawnAreaDimensionY, spawnAreaDimensionZ;
+    uint32_t spawnPlacementId;
+    uint32_t spawnRegionShapeId; /* 0 = random fill, otherwise filled box */
+    uint32_t spawnSizeIndex;
+    uint32_t spawnDensityIndex;  /* density (i+1)/16 */
+    uint32_t runSeedIndex;
+    uint32_t partitionIndex;
+    uint32_t partitionCount;
+} cave_chunk_config;
+
+/* Per-tick statistics: the reference GridSnapshot plus fields the reference does not
+ * compute. population = non-zero cells after the tick; changed = cells whose state
+ * changed (= born + dying); bbox of non-zero cells after the tick (min = 0xFFFFFFFF and
+ * max = 0 on every axis when no cell is non-zero). */
+typedef struct {
+    cave_grid_snapshot snapshot;
+    uint32_t population;
+    uint32_t changed;
+    uint32_t bbox_min[3];
+    uint32_t bbox_max[3];
+} cave_tick_stats;
+
+/* ---- context ------------------------------------------------------------------------ */
+typedef struct cave_ctx cave_ctx;
+
+/* Replaces DeviceContext construction for the search path (src/vulkan/deviceContext.*). */
+cave_status cave_ctx_create(int device, cave_ctx** out);
+void cave_ctx_destroy(cave_ctx* ctx);
+const char* cave_status_string(cave_status s);
+const char* cave_last_error(const cave_ctx* ctx);
+/* Blocks until all work queued on the context's stream is done. */
+cave_status cave_ctx_synchronize(cave_ctx* ctx);
+
+/* ---- grids --------------------------------------------------------------------------- */
+typedef struct cave_grid cave_grid;
+
+/* Replaces the per-slot cellsIn/cellsOut/initialCells buffers of
+ * SearchSystem::BuildBuffers (searchSystem.cpp:126-394). The grid holds two device copies of
+ * the cells (ping-pong); the "current" one is what upload/download/step see. */
+cave_status cave_grid_create(cave_ctx* ctx, uint32_t X, uint32_t Y, uint32_t Z, cave_grid** out);
+void cave_grid_destroy(cave_grid* g);
+/* Number of uint32 words in the padded nibble layout: ceil(X/8)*Y*Z. */
+uint64_t cave_grid_words(uint32_t X, uint32_t Y, uint32_t Z);
+cave_status cave_grid_upload(cave_grid* g, const uint32_t* words, uint64_t nwords);
+cave_status cave_grid_download(cave_grid* g, uint32_t* words, uint64_t nwords);
+
+/* Initial cells on the device, same cells as searchSystem.cpp:219-306 for `chunk` and
+ * `maxCellState` (random fill when spawnRegionShapeId == 0, density from spawnDensityIndex). */
+cave_status cave_grid_seed(cave_grid* g, const cave_chunk_config* chunk, uint32_t maxCellState);
+/* Same hash and spawn box with an explicit fill threshold: a box cell is alive iff
+ * cellHash(x,y,z,seed) < threshold; threshold = 2^32 fills the whole box. This expresses
+ * fills such as 0.30 (threshold (uint32)((double)0.30f * 2^32)) that the 1/16-step density
+ * index cannot. */
+cave_status cave_grid_seed_threshold(cave_grid* g, uint32_t spawnX, uint32_t spawnY, uint32_t spawnZ,
+                                     uint64_t threshold, uint32_t runSeedIndex, uint32_t maxCellState);
+
+/* ---- plain path: one launch per tick ------------------------------------------------- */
+/* Replaces one Phase-1 + Phase-2 + Phase-3 pass of SearchSystem::SubmitNextTick
+ * (searchSystem.cpp:541-616): searchSimulationCube.slang computeMain over the grid, its
+ * GridSnapshot reduction, and the cellsOut -> cellsIn copy (here a ping-pong swap).
+ * Runs `nticks` launches; per_tick (host array of nticks, may be NULL) receives each
+ * tick's statistics. validBitmasks/nValid are the K-index table (binding 4, used when
+ * maxRuleBits > 0; EnumerateValidBitmasks order). Rule indices outside the table are
+ * rejected with CAVE_ERR_INVALID_ARG. */
+cave_status cave_step(cave_grid* g, const cave_sim_params* params, const uint64_t* validBitmasks,
+                      uint32_t nValid, uint32_t maxRuleBits, uint32_t nticks, cave_tick_stats* per_tick);
+
+/* ---- streaming path: many ticks in the library's bit-plane layout -------------------- */
+/* Same results as cave_step for the same inputs (every cell, every statistic), computed by
+ * the z-slab streaming kernel: the grid is converted to a bit-plane layout once, stepped
+ * nticks times (one launch per tick, captured in a CUDA graph) and converted back. The
+ * GridInfo of the manager shader (searchManager.slang:98-139) for those ticks is returned in
+ * *info (may be NULL) with maxTicks as MAX_NUMBER_OF_TICKS_TO_SURVIVE; the run does not stop
+ * on status > 0 (raw stepping). */
+cave_status cave_run(cave_grid* g, const cave_sim_params* params, const uint64_t* validBitmasks,
+                     uint32_t nValid, uint32_t maxRuleBits, uint32_t nticks, uint32_t maxTicks,
+                     cave_tick_stats* per_tick, cave_grid_info* info);
+
+/* ---- manager (host restatement) ------------------------------------------------------ */
+/* One dispatch of searchManager.slang computeMain (:98-149) including NextPermutation
+ * (:56-96), for callers that drive the plain path themselves. */
+void cave_manager_update(const cave_grid_snapshot* snapshot, cave_grid_info* info, cave_sim_params* perms,
+                         uint64_t maxPermutation, uint64_t survivalEndPermutation, uint32_t maxTicks,
+                         cave_grid_info* infoCopy, cave_sim_params* permsCopy);
+
+/* ---- valid bitmasks (permutationMath.h:101-128) ---------------------------------------- */
+/* Returns the number of masks with 1..maxBits bits set among the low neighborCount bits and
+ * writes up to cap of them, sorted ascending. */
+uint64_t cave_enumerate_valid_bitmasks(uint32_t neighborCount, uint32_t maxBits, uint64_t* out, uint64_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CAVE_CA_H */
