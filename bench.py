@@ -1,0 +1,345 @@
+#!/usr/bin/env python
+"""bench.py -- throughput of the B200 CA stepping path on the reference's headline workloads.
+
+Default workload (one GPU): a 512^3 grid, Moore-26 neighbourhood, C = 16 states (maxCellState
+15), survive {4,5}, birth {5}, 40% of the whole volume seeded alive by the reference's cell
+hash (seed 0), 1000 ticks with statistics every tick. One "step" is one full 1000-tick run
+through the C ABI (cave_run: nibble layout in HBM -> bit-plane layout -> 1000 tick launches ->
+back). `value` is cell-updates/s with the grid already resident in HBM; `e2e` is the same
+through cave_run_host with the grid read from and written back to pinned host memory.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl reference]
+
+Under torchrun (N > 1) every rank runs an independent replica (a single grid does not shard
+without a halo exchange the reference does not do in search mode); value = all ranks' cell
+updates / max over ranks of the device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (edge, ticks)
+    "large512": (512, 1000),
+    "large256": (256, 1000),
+    "large1024": (1024, 200),
+}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="large512")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ticks", type=int, default=0, help="override the workload's tick count (profiling runs)")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------- helpers
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for i, n in enumerate(names):
+                    if r[5 + i].strip().lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        os.unlink(self.f.name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic(kernel_key):
+    """DRAM bytes per launch from the committed ncu summary (profiles/<kernel_key>.md)."""
+    p = os.path.join(ROOT, "profiles", f"{kernel_key}.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg, local):
+    import torch
+
+    torch.cuda.synchronize(local)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize(local)
+
+
+def max_over_ranks(pg, local, v):
+    if not pg:
+        return v
+    import torch
+
+    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(pg, local, v):
+    if not pg:
+        return v
+    import torch
+
+    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------------------- CPU baseline
+def cpu_baseline_large(G, init, params, budget_s=12.0):
+    """The oracle's OpenMP step (bit-identical to the literal restatement) on the same grid."""
+    import oracle as O
+
+    cores = os.cpu_count() or 1
+    cells = init
+    t0 = time.perf_counter()
+    ticks = 0
+    while True:
+        cells, _ = O.step_fast(G, G, G, params, cells, nthreads=cores)
+        ticks += 1
+        el = time.perf_counter() - t0
+        if el > budget_s or ticks >= 50:
+            break
+    return {"value": G ** 3 * ticks / el, "unit": "cell-updates/s", "cores": cores, "kind": "port",
+            "sample": f"{ticks} ticks of the {G}^3 grid (of {WORKLOADS.get(f'large{G}', (G, 0))[1]}), oracle "
+                      f"OpenMP z-slab step, {el:.1f} s"}
+
+
+# ----------------------------------------------------------------------------- workloads
+def large_workload(args, world, rank, local, pg):
+    import numpy as np
+    import torch
+
+    import cave_b200 as cb
+    import oracle as O
+
+    G, T = WORKLOADS[args.workload]
+    T = args.ticks or T
+    cells_per_step = G ** 3 * T
+    thr = O.threshold_from_float(0.40)
+    params_np = O.make_params(15, 0x7, 0x10, 0x18)
+    params = cb.SimParams(*[int(v) for v in params_np])
+    ctx = cb.Context(local)
+    ctx.set_timing(True)
+    g = cb.Grid(ctx, G, G, G)
+    g.seed_threshold((G, G, G), thr, 0, 15)
+    init_host = g.download()
+    words = init_host.size
+    pin_in = torch.from_numpy(init_host.view(np.int32)).pin_memory()
+    pin_out = torch.empty(words, dtype=torch.int32).pin_memory()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=f"cuda:{local}")  # 256 MiB > L2
+
+    def reset():
+        g.upload(init_host)
+        flush.zero_()
+        torch.cuda.synchronize(local)
+
+    for _ in range(args.warmup):
+        reset()
+        g.run(params, T, T, stats=True)
+    barrier(pg, local)
+    dev_ms, tick_ms, conv_ms, launches = [], [], [], 0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            reset()
+            g.run(params, T, T, stats=True)
+            t = ctx.last_timing()
+            dev_ms.append(t.total_ms)
+            tick_ms.append(t.tick_ms)
+            conv_ms.append(t.convert_ms)
+            launches += t.launches
+        barrier(pg, local)
+    clocks = clk.summary()
+    # end-to-end through the C ABI with host buffers
+    e2e_ms = []
+    for i in range(0 if args.no_e2e else args.steps + 1):
+        flush.zero_()
+        torch.cuda.synchronize(local)
+        g.run_host(pin_in.data_ptr(), pin_out.data_ptr(), params, T, T, stats=True)
+        if i > 0:
+            e2e_ms.append(ctx.last_timing().total_ms)
+    barrier(pg, local)
+
+    tot_dev = max_over_ranks(pg, local, sum(dev_ms))
+    tot_e2e = max_over_ranks(pg, local, sum(e2e_ms)) if e2e_ms else float("nan")
+    tot_tick = max_over_ranks(pg, local, sum(tick_ms))
+    value = world * cells_per_step * args.steps / (tot_dev / 1e3)
+    e2e_value = world * cells_per_step * args.steps / (tot_e2e / 1e3)
+    per_launch_s = (tot_tick / 1e3) / (T * args.steps)
+    alg_bytes = G ** 3  # 1 byte per cell update: 0.5 B read + 0.5 B written
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / per_launch_s / 1e9
+    traffic = committed_traffic(f"stream_tick_{G}")
+    line = {
+        "metric": "cell-updates/s",
+        "value": value,
+        "unit": "cell-updates/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": tot_dev / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u4 (packed nibble states, bit-sliced integer logic)",
+        "data": "synthetic: reference cell hash (searchSystem.cpp:244-262), seed 0, 40% fill of the whole volume",
+        "config": {"workload": f"{G}^3 Moore-26, C=16 (maxCellState 15), survive {{4,5}} birth {{5}}, "
+                               f"{T} ticks, stats every tick", "grid": [G, G, G], "ticks": T,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "256 MiB buffer written between timed steps (a step is one whole run; within a run each "
+                         "tick reads the previous tick's output)"},
+        "tick_kernel_us": per_launch_s * 1e6,
+        "convert_ms_per_step": sum(conv_ms) / len(conv_ms),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "traffic": traffic,
+                     "note": "algorithmic bytes = 1 B per cell update (packed 4-bit state read once, written once)"},
+        "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": int(words * 4),
+                "d2h_bytes_per_step": int(words * 4 + T * 48)},
+        "gpu_launches": int(sum_over_ranks(pg, local, launches)),
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_large(G, init_host, params_np)
+    g.close()
+    ctx.close()
+    return line
+
+
+def reference_arm(args, world, rank, local, pg):
+    """The oracle port of the reference's CPU-free arithmetic on the host cores (no CPU stepping
+    exists in the reference; its GPU path needs Vulkan, which this box does not have)."""
+    import oracle as O
+
+    if rank != 0:
+        return None
+    G, T = WORKLOADS[args.workload]
+    params = O.make_params(15, 0x7, 0x10, 0x18)
+    init = O.seed(G, G, G, random=True, threshold=O.threshold_from_float(0.40), run_seed=0, max_cell_state=15)
+    cores = os.cpu_count() or 1
+    ticks_per_step = 1
+    cells = init
+    for _ in range(args.warmup):
+        cells, _ = O.step_fast(G, G, G, params, cells, nthreads=cores)
+    t0 = time.perf_counter()
+    for _ in range(args.steps * ticks_per_step):
+        cells, _ = O.step_fast(G, G, G, params, cells, nthreads=cores)
+    el = time.perf_counter() - t0
+    v = G ** 3 * args.steps * ticks_per_step / el
+    return {
+        "impl": "reference", "metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u4", "data": "synthetic (same seed and fill)",
+        "config": {"workload": f"{G}^3 Moore-26, C=16, survive {{4,5}} birth {{5}}; one tick per step "
+                               f"(bounded sample of the {T}-tick run)", "grid": [G, G, G]},
+        "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} ticks of {G}^3 after {args.warmup} warm-up ticks"},
+        "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        # rank 0 alone runs the CPU arm; other ranks exit without work (no process group).
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        line = reference_arm(args, world, rank, 0, None)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    world, rank, local, pg = dist_setup(args)
+    line = large_workload(args, world, rank, local, pg)
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -63,6 +63,11 @@ class TickStats(ctypes.Structure):
                                            tuple(self.bbox_max))
 
 
+class Timing(ctypes.Structure):
+    _fields_ = [("ticks", u32), ("launches", u32), ("tick_ms", ctypes.c_float), ("convert_ms", ctypes.c_float),
+                ("total_ms", ctypes.c_float)]
+
+
 class CaveError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"{msg} (status {code})")
@@ -78,6 +83,10 @@ _SIGS = {
     "cave_status_string": (ctypes.c_char_p, [i32]),
     "cave_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "cave_ctx_synchronize": (i32, [ctypes.c_void_p]),
+    "cave_ctx_set_timing": (i32, [ctypes.c_void_p, i32]),
+    "cave_ctx_last_timing": (i32, [ctypes.c_void_p, P(Timing)]),
+    "cave_run_host": (i32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, u64, P(SimParams), P(u64), u32, u32,
+                            u32, u32, P(TickStats), P(GridInfo)]),
     "cave_grid_create": (i32, [ctypes.c_void_p, u32, u32, u32, P(ctypes.c_void_p)]),
     "cave_grid_destroy": (None, [ctypes.c_void_p]),
     "cave_grid_words": (u64, [u32, u32, u32]),
@@ -155,6 +164,14 @@ class Context:
     def synchronize(self):
         self.check(lib().cave_ctx_synchronize(self.h), "cave_ctx_synchronize")
 
+    def set_timing(self, enable=True):
+        self.check(lib().cave_ctx_set_timing(self.h, 1 if enable else 0), "cave_ctx_set_timing")
+
+    def last_timing(self) -> Timing:
+        t = Timing()
+        self.check(lib().cave_ctx_last_timing(self.h, ctypes.byref(t)), "cave_ctx_last_timing")
+        return t
+
     def close(self):
         if self.h:
             lib().cave_ctx_destroy(self.h)
@@ -220,6 +237,18 @@ class Grid:
         self.ctx.check(lib().cave_run(self.h, ctypes.byref(params), _u64p(v), 0 if v is None else v.size,
                                       max_rule_bits, nticks, nticks if max_ticks is None else max_ticks, pt,
                                       ctypes.byref(info)), "cave_run")
+        return ([pt[i] for i in range(nticks)] if stats else None), info
+
+    def run_host(self, in_ptr, out_ptr, params: SimParams, nticks, max_ticks=None, valid=None, max_rule_bits=0,
+                 stats=True):
+        """Streaming path with host buffers (raw pointers to `words` uint32 each, ideally pinned)."""
+        v = None if valid is None else np.ascontiguousarray(valid, dtype=np.uint64)
+        pt = (TickStats * max(nticks, 1))() if stats else None
+        info = GridInfo()
+        self.ctx.check(lib().cave_run_host(self.h, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr), self.words,
+                                           ctypes.byref(params), _u64p(v), 0 if v is None else v.size, max_rule_bits,
+                                           nticks, nticks if max_ticks is None else max_ticks, pt,
+                                           ctypes.byref(info)), "cave_run_host")
         return ([pt[i] for i in range(nticks)] if stats else None), info
 
 

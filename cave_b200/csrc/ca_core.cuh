@@ -15,7 +15,7 @@
 // Neighbour counting is done on alive bit-planes with full adders (XOR3 / MAJ, one LOP3
 // each). The count is formed as Bn = sum over the 3x3 (y,z) rows of per-row terms, with
 // the reference's delta sets (cube.slang:7-21) split by row class:
-//   centre row (y,z)        : faces along x            -> L+R
+//   centre row (y,z)           : faces along x (dx=+-1)
 //   face rows (y+-1,z),(y,z+-1): face (dx=0) + edges (dx=+-1)
 //   diagonal rows (y+-1,z+-1)  : edge (dx=0) + corners (dx=+-1)
 // For neighbourhoods that contain faces the centre row contributes H = L+A+R, so Bn counts
@@ -40,7 +40,7 @@ __device__ __forceinline__ void add3(const uint32_t* a, const uint32_t* b, const
     uint32_t s[N + 1], k[N + 1];
 #pragma unroll
     for (int i = 0; i < N; i++) {
-        uint32_t x = i < NA ? a[i] : 0u, y = i < NB ? b[i] : 0u, z = i < NC ? c[i] : 0u;
+        const uint32_t x = i < NA ? a[i] : 0u, y = i < NB ? b[i] : 0u, z = i < NC ? c[i] : 0u;
         s[i] = xor3(x, y, z);
         k[i] = maj3(x, y, z);
     }
@@ -50,8 +50,8 @@ __device__ __forceinline__ void add3(const uint32_t* a, const uint32_t* b, const
     uint32_t carry = 0u;
 #pragma unroll
     for (int i = 0; i < NO; i++) {
-        uint32_t x = i <= N ? s[i] : 0u;
-        uint32_t y = (i >= 1 && i - 1 <= N) ? k[i - 1] : 0u;
+        const uint32_t x = i <= N ? s[i] : 0u;
+        const uint32_t y = (i >= 1 && i - 1 <= N) ? k[i - 1] : 0u;
         if (i == 0) {
             out[0] = x;
         } else {
@@ -69,8 +69,8 @@ __device__ __forceinline__ uint32_t lut_tree(const uint32_t* c, uint32_t lut) {
     uint32_t v[NL / 2];
 #pragma unroll
     for (int j = 0; j < NL / 2; j++) {
-        uint32_t t0 = 0u - ((lut >> (2 * j)) & 1u);
-        uint32_t t1 = 0u - ((lut >> (2 * j + 1)) & 1u);
+        const uint32_t t0 = 0u - ((lut >> (2 * j)) & 1u);
+        const uint32_t t1 = 0u - ((lut >> (2 * j + 1)) & 1u);
         v[j] = (c[0] & t1) | (~c[0] & t0);
     }
 #pragma unroll
@@ -81,21 +81,20 @@ __device__ __forceinline__ uint32_t lut_tree(const uint32_t* c, uint32_t lut) {
     return v[0];
 }
 
-// (survive-hit, birth-hit) planes for count planes c.
-template <int NBITS, bool SPARSE>
+// (survive-hit, birth-hit) planes for count planes c. NT = number of sparse terms the rule
+// was built with (1..kMaxTerms), or 0 for the mux-tree evaluation of the two tables.
+template <int NBITS, int NT>
 __device__ __forceinline__ void eval_rule(const uint32_t* c, const DeviceRule& r, uint32_t& hs, uint32_t& hb) {
-    if constexpr (SPARSE) {
+    if constexpr (NT > 0) {
         uint32_t as = 0u, ab = 0u;
 #pragma unroll
-        for (int t = 0; t < kMaxTerms; t++) {
-            if (t < (int)r.nterms) {
-                const RuleTerm& T = r.terms[t];
-                uint32_t e = (c[0] ^ T.nk[0]) & (c[1] ^ T.nk[1]) & (c[2] ^ T.nk[2]);
-                if (NBITS > 3) e &= (c[3] ^ T.nk[3]);
-                if (NBITS > 4) e &= (c[4] ^ T.nk[4]);
-                as |= e & T.sm;
-                ab |= e & T.bm;
-            }
+        for (int t = 0; t < NT; t++) {
+            const RuleTerm& T = r.terms[t];
+            uint32_t e = (c[0] ^ T.nk[0]) & (c[1] ^ T.nk[1]) & (c[2] ^ T.nk[2]);
+            if constexpr (NBITS > 3) e &= (c[3] ^ T.nk[3]);
+            if constexpr (NBITS > 4) e &= (c[4] ^ T.nk[4]);
+            as |= e & T.sm;
+            ab |= e & T.bm;
         }
         hs = as;
         hb = ab;
@@ -107,17 +106,27 @@ __device__ __forceinline__ void eval_rule(const uint32_t* c, const DeviceRule& r
 
 // ---------------------------------------------------------------- per-row terms
 __device__ __forceinline__ uint32_t alive_plane(uint4 s, const DeviceRule& r) {
-    uint32_t d = (s.x ^ r.m[0]) | (s.y ^ r.m[1]) | (s.z ^ r.m[2]) | (s.w ^ r.m[3]);
+    const uint32_t d = (s.x ^ r.m[0]) | (s.y ^ r.m[1]) | (s.z ^ r.m[2]) | (s.w ^ r.m[3]);
     return ~d & r.alive_ok;
 }
 
-struct Row {           // alive bits and their x-neighbours for one strip of one row
-    uint32_t a, l, r;  // l: bit j = alive(x-1), r: bit j = alive(x+1)
+// Sums of one strip of one row, formed once when the row is read: a = alive bits,
+// h = l + a + r (2 planes), lr = l + r (2 planes), with l/r the x-1 / x+1 alive bits.
+struct Row {
+    uint32_t a, h0, h1, lr0, lr1;
 };
 
-// H = l + a + r  (2 planes), LR = l + r (2 planes)
-__device__ __forceinline__ void hsum(const Row& w, uint32_t* h) { h[0] = xor3(w.l, w.a, w.r); h[1] = maj3(w.l, w.a, w.r); }
-__device__ __forceinline__ void lrsum(const Row& w, uint32_t* h) { h[0] = w.l ^ w.r; h[1] = w.l & w.r; }
+__device__ __forceinline__ Row make_row(uint32_t a, uint32_t a_left, uint32_t a_right) {
+    const uint32_t l = __funnelshift_l(a_left, a, 1);   // bit j = alive(x-1)
+    const uint32_t r = __funnelshift_r(a, a_right, 1);  // bit j = alive(x+1)
+    Row w;
+    w.a = a;
+    w.h0 = xor3(l, a, r);
+    w.h1 = maj3(l, a, r);
+    w.lr0 = l ^ r;
+    w.lr1 = l & r;
+    return w;
+}
 
 // Column partial sums for neighbourhood NB from the column's rows at z-1 (m), z (c), z+1 (p):
 //   pc: contribution when this column is the output's own column
@@ -131,12 +140,10 @@ template <> struct Partials<0> {  // no neighbourhood selected: every count is 0
         ps[0] = 0u;
     }
 };
-
 template <> struct Partials<1> {  // F: centre H, face rows A
     static constexpr int NC = 3, NS = 1;
     __device__ static void make(const Row& m, const Row& c, const Row& p, uint32_t* pc, uint32_t* ps) {
-        uint32_t h[2]; hsum(c, h);
-        uint32_t am[1] = {m.a}, ap[1] = {p.a};
+        const uint32_t h[2] = {c.h0, c.h1}, am[1] = {m.a}, ap[1] = {p.a};
         add3<2, 1, 1, 3>(h, am, ap, pc);
         ps[0] = c.a;
     }
@@ -144,27 +151,25 @@ template <> struct Partials<1> {  // F: centre H, face rows A
 template <> struct Partials<2> {  // E: face rows LR, diagonal rows A
     static constexpr int NC = 3, NS = 3;
     __device__ static void make(const Row& m, const Row& c, const Row& p, uint32_t* pc, uint32_t* ps) {
-        uint32_t lm[2], lp[2], lc[2]; lrsum(m, lm); lrsum(p, lp); lrsum(c, lc);
-        uint32_t z[1] = {0u};
+        const uint32_t lm[2] = {m.lr0, m.lr1}, lp[2] = {p.lr0, p.lr1}, lc[2] = {c.lr0, c.lr1}, z[1] = {0u};
         add3<2, 2, 1, 3>(lm, lp, z, pc);
-        uint32_t am[1] = {m.a}, ap[1] = {p.a};
+        const uint32_t am[1] = {m.a}, ap[1] = {p.a};
         add3<2, 1, 1, 3>(lc, am, ap, ps);
     }
 };
 template <> struct Partials<3> {  // FE: centre H, face rows H, diagonal rows A
     static constexpr int NC = 4, NS = 3;
     __device__ static void make(const Row& m, const Row& c, const Row& p, uint32_t* pc, uint32_t* ps) {
-        uint32_t hm[2], hc[2], hp[2]; hsum(m, hm); hsum(c, hc); hsum(p, hp);
+        const uint32_t hm[2] = {m.h0, m.h1}, hc[2] = {c.h0, c.h1}, hp[2] = {p.h0, p.h1};
         add3<2, 2, 2, 4>(hm, hc, hp, pc);
-        uint32_t am[1] = {m.a}, ap[1] = {p.a};
+        const uint32_t am[1] = {m.a}, ap[1] = {p.a};
         add3<2, 1, 1, 3>(hc, am, ap, ps);
     }
 };
 template <> struct Partials<4> {  // C: diagonal rows LR
     static constexpr int NC = 1, NS = 3;
     __device__ static void make(const Row& m, const Row& c, const Row& p, uint32_t* pc, uint32_t* ps) {
-        uint32_t lm[2], lp[2]; lrsum(m, lm); lrsum(p, lp);
-        uint32_t z[1] = {0u};
+        const uint32_t lm[2] = {m.lr0, m.lr1}, lp[2] = {p.lr0, p.lr1}, z[1] = {0u};
         add3<2, 2, 1, 3>(lm, lp, z, ps);
         pc[0] = 0u;
     }
@@ -172,28 +177,25 @@ template <> struct Partials<4> {  // C: diagonal rows LR
 template <> struct Partials<5> {  // FC: centre H, face rows A, diagonal rows LR
     static constexpr int NC = 3, NS = 3;
     __device__ static void make(const Row& m, const Row& c, const Row& p, uint32_t* pc, uint32_t* ps) {
-        uint32_t hc[2]; hsum(c, hc);
-        uint32_t am[1] = {m.a}, ap[1] = {p.a};
+        const uint32_t hc[2] = {c.h0, c.h1}, am[1] = {m.a}, ap[1] = {p.a};
         add3<2, 1, 1, 3>(hc, am, ap, pc);
-        uint32_t lm[2], lp[2]; lrsum(m, lm); lrsum(p, lp);
-        uint32_t ac[1] = {c.a};
+        const uint32_t lm[2] = {m.lr0, m.lr1}, lp[2] = {p.lr0, p.lr1}, ac[1] = {c.a};
         add3<2, 2, 1, 3>(lm, lp, ac, ps);
     }
 };
 template <> struct Partials<6> {  // EC: face rows LR, diagonal rows H
     static constexpr int NC = 3, NS = 4;
     __device__ static void make(const Row& m, const Row& c, const Row& p, uint32_t* pc, uint32_t* ps) {
-        uint32_t lm[2], lp[2], lc[2]; lrsum(m, lm); lrsum(p, lp); lrsum(c, lc);
-        uint32_t z[1] = {0u};
+        const uint32_t lm[2] = {m.lr0, m.lr1}, lp[2] = {p.lr0, p.lr1}, lc[2] = {c.lr0, c.lr1}, z[1] = {0u};
         add3<2, 2, 1, 3>(lm, lp, z, pc);
-        uint32_t hm[2], hp[2]; hsum(m, hm); hsum(p, hp);
+        const uint32_t hm[2] = {m.h0, m.h1}, hp[2] = {p.h0, p.h1};
         add3<2, 2, 2, 4>(lc, hm, hp, ps);
     }
 };
 template <> struct Partials<7> {  // FEC: every row H (pc == ps)
     static constexpr int NC = 4, NS = 4;
     __device__ static void make(const Row& m, const Row& c, const Row& p, uint32_t* pc, uint32_t* ps) {
-        uint32_t hm[2], hc[2], hp[2]; hsum(m, hm); hsum(c, hc); hsum(p, hp);
+        const uint32_t hm[2] = {m.h0, m.h1}, hc[2] = {c.h0, c.h1}, hp[2] = {p.h0, p.h1};
         add3<2, 2, 2, 4>(hm, hc, hp, pc);
 #pragma unroll
         for (int i = 0; i < 4; i++) ps[i] = pc[i];
@@ -210,61 +212,53 @@ __device__ __forceinline__ void combine(const uint32_t* pc, const uint32_t* psm,
 // ---------------------------------------------------------------- state update + stats
 struct TickAcc {  // per-thread accumulators for one tick
     uint32_t surviving, born, zero, population;
-    uint32_t bmin[3], bmax[3];
+    uint32_t zmin, zmax;  // z-extent of the thread's non-zero strips
     __device__ void reset() {
         surviving = born = zero = population = 0u;
-        bmin[0] = bmin[1] = bmin[2] = 0xFFFFFFFFu;
-        bmax[0] = bmax[1] = bmax[2] = 0u;
+        zmin = 0xFFFFFFFFu;
+        zmax = 0u;
     }
 };
 
-// New state of one strip. s: current state planes; a: its alive plane; valid: cells < X.
-template <int NB, bool SPARSE>
+// New state of one strip. s: current state planes; a: its alive plane; valid: cells < X;
+// xbits accumulates the OR of the strip's non-zero masks (its x-extent). The statistics are
+// accumulated only when `count` is set (strips this thread owns, not halo copies).
+template <int NB, int NT>
 __device__ __forceinline__ uint4 update_strip(uint4 s, uint32_t a, const uint32_t* cnt, uint32_t valid,
-                                              const DeviceRule& r, TickAcc& acc, uint32_t x0, uint32_t y,
-                                              uint32_t z) {
+                                              const DeviceRule& r, TickAcc& acc, uint32_t& xbits, uint32_t z,
+                                              bool count = true) {
     uint32_t hs, hb;
-    eval_rule<count_bits(NB), SPARSE>(cnt, r, hs, hb);
+    eval_rule<count_bits(NB), NT>(cnt, r, hs, hb);
     const uint32_t nz = s.x | s.y | s.z | s.w;
     const uint32_t zero = ~nz & valid;
     const uint32_t sv = a & hs;
     const uint32_t bn = zero & hb;
     const uint32_t set = sv | bn;
-    const uint32_t keep = nz & ~set;
-    // s - 1 for non-zero cells (borrow chain), maxcs where set, 0 for dead cells
-    const uint32_t b1 = ~s.x;
-    const uint32_t b2 = b1 & ~s.y;
+    // d = s - 1 for non-zero cells, 0 for zero cells (borrow chain masked by nz); then each
+    // plane is set ? bit of maxcs : d (one 3-input select per plane)
+    const uint32_t b2 = ~s.x & ~s.y;
     const uint32_t b3 = b2 & ~s.z;
+    const uint32_t d0 = nz & ~s.x;
+    const uint32_t d1 = nz & ~(s.y ^ s.x);
+    const uint32_t d2 = nz & (s.z ^ b2);
+    const uint32_t d3 = nz & (s.w ^ b3);
     uint4 n;
-    n.x = (set & r.m[0]) | (keep & ~s.x);
-    n.y = (set & r.m[1]) | (keep & (s.y ^ b1));
-    n.z = (set & r.m[2]) | (keep & (s.z ^ b2));
-    n.w = (set & r.m[3]) | (keep & (s.w ^ b3));
-    acc.surviving += __popc(sv);
-    acc.born += __popc(bn);
-    acc.zero += __popc(zero);
-    const uint32_t nn = n.x | n.y | n.z | n.w;
-    if (nn) {
+    n.x = (set & r.m[0]) | (~set & d0);
+    n.y = (set & r.m[1]) | (~set & d1);
+    n.z = (set & r.m[2]) | (~set & d2);
+    n.w = (set & r.m[3]) | (~set & d3);
+    if (count) {
+        acc.surviving += __popc(sv);
+        acc.born += __popc(bn);
+        acc.zero += __popc(zero);
+        const uint32_t nn = n.x | n.y | n.z | n.w;
         acc.population += __popc(nn);
-        const uint32_t lo = x0 + (uint32_t)(__ffs(nn) - 1);
-        const uint32_t hi = x0 + 31u - (uint32_t)__clz(nn);
-        acc.bmin[0] = min(acc.bmin[0], lo);
-        acc.bmax[0] = max(acc.bmax[0], hi);
-        acc.bmin[1] = min(acc.bmin[1], y);
-        acc.bmax[1] = max(acc.bmax[1], y);
-        acc.bmin[2] = min(acc.bmin[2], z);
-        acc.bmax[2] = max(acc.bmax[2], z);
+        xbits |= nn;
+        const bool any = nn != 0u;
+        acc.zmin = any ? min(acc.zmin, z) : acc.zmin;
+        acc.zmax = any ? max(acc.zmax, z) : acc.zmax;
     }
     return n;
-}
-
-// x-neighbour words for the alive plane of a strip, given the neighbouring strips' planes.
-__device__ __forceinline__ Row make_row(uint32_t a, uint32_t a_left, uint32_t a_right) {
-    Row w;
-    w.a = a;
-    w.l = (a << 1) | (a_left >> 31);
-    w.r = (a >> 1) | (a_right << 31);
-    return w;
 }
 
 }  // namespace cave

@@ -18,7 +18,8 @@ struct RuleTerm {
 };
 static_assert(sizeof(RuleTerm) == 32, "RuleTerm is two 16-byte words");
 
-constexpr int kMaxTerms = 8;  // the sparse path handles rules with <= kMaxTerms distinct counts
+constexpr int kMaxTerms = 8;        // capacity of DeviceRule::terms
+constexpr int kMaxSparseTerms = 4;  // the kernels' sparse evaluation handles up to this many terms
 
 // Decoded rule for one simulation, in the form the kernels consume.
 //   lut_s: bit b set  <=> an alive cell whose row-sum count is b survives

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -27,6 +28,29 @@ cave_status check_cuda(cave_ctx* ctx, cudaError_t e, const char* what) {
     if (e == cudaSuccess) return CAVE_OK;
     const cave_status code = (e == cudaErrorMemoryAllocation) ? CAVE_ERR_OUT_OF_MEMORY : CAVE_ERR_CUDA;
     return set_error(ctx, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Timing events of one call: 0 start, 1 before conversion, 2 first tick, 3 after the last
+// tick, 4 after conversion back, 5 end.
+static void record(cave_ctx* ctx, int i) {
+    if (ctx->timing) cudaEventRecord(ctx->ev[i], ctx->stream);
+}
+
+static void finish_timing(cave_ctx* ctx, uint32_t ticks, uint32_t launches, bool converted) {
+    if (!ctx->timing) return;
+    cave_timing t{};
+    t.ticks = ticks;
+    t.launches = launches;
+    float a = 0, b = 0, c = 0;
+    cudaEventElapsedTime(&a, ctx->ev[2], ctx->ev[3]);
+    if (converted) {
+        cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
+        cudaEventElapsedTime(&c, ctx->ev[3], ctx->ev[4]);
+    }
+    t.tick_ms = a;
+    t.convert_ms = b + c;
+    cudaEventElapsedTime(&t.total_ms, ctx->ev[0], ctx->ev[5]);
+    ctx->last_timing = t;
 }
 
 static uint32_t resolve_spawn(uint32_t axis, uint32_t sizeIndex) {  // searchSystem.cpp:226-232
@@ -147,6 +171,8 @@ void cave_ctx_destroy(cave_ctx* ctx) {
         cudaStreamSynchronize(ctx->stream);
         cudaStreamDestroy(ctx->stream);
     }
+    for (auto& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
     delete ctx;
 }
 
@@ -287,33 +313,82 @@ cave_status cave_step(cave_grid* g, const cave_sim_params* params, const uint64_
     s.run_manager = 0;
     s.per_tick = dticks;
     cudaError_t e = cudaMemcpyAsync(g->slot, &s, sizeof(s), cudaMemcpyHostToDevice, ctx->stream);
+    record(ctx, 0);
+    record(ctx, 2);
     for (uint32_t t = 0; t < nticks && e == cudaSuccess; t++) {
         e = launch_plain_step(g->nib[g->cur], g->nib[g->cur ^ 1], g->X, g->Y, g->Z, g->slot, tab.p, nValid,
                               maxRuleBits, ctx->stream);
         g->cur ^= 1;
     }
+    record(ctx, 3);
     if (e == cudaSuccess && per_tick)
         e = cudaMemcpyAsync(per_tick, dticks, sizeof(cave_tick_stats) * nticks, cudaMemcpyDeviceToHost, ctx->stream);
     PlainSlot back;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&back, g->slot, sizeof(back), cudaMemcpyDeviceToHost, ctx->stream);
+    record(ctx, 5);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     cudaFree(dticks);
     if (e != cudaSuccess) return check_cuda(ctx, e, "cave_step");
+    finish_timing(ctx, nticks, nticks, false);
     if (back.error) return set_error(ctx, CAVE_ERR_INTERNAL, "plain kernel raised an error flag");
     return CAVE_OK;
 }
 
+static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* host_out, const cave_sim_params* params,
+                            const uint64_t* validBitmasks, uint32_t nValid, uint32_t maxRuleBits, uint32_t nticks,
+                            uint32_t maxTicks, cave_tick_stats* per_tick, cave_grid_info* info);
+
 cave_status cave_run(cave_grid* g, const cave_sim_params* params, const uint64_t* validBitmasks, uint32_t nValid,
                      uint32_t maxRuleBits, uint32_t nticks, uint32_t maxTicks, cave_tick_stats* per_tick,
                      cave_grid_info* info) {
+    return run_impl(g, nullptr, nullptr, params, validBitmasks, nValid, maxRuleBits, nticks, maxTicks, per_tick, info);
+}
+
+cave_status cave_run_host(cave_grid* g, const uint32_t* in_words, uint32_t* out_words, uint64_t nwords,
+                          const cave_sim_params* params, const uint64_t* validBitmasks, uint32_t nValid,
+                          uint32_t maxRuleBits, uint32_t nticks, uint32_t maxTicks, cave_tick_stats* per_tick,
+                          cave_grid_info* info) {
+    if (!g || !in_words || !out_words || nwords != g->words) return CAVE_ERR_INVALID_ARG;
+    return run_impl(g, in_words, out_words, params, validBitmasks, nValid, maxRuleBits, nticks, maxTicks, per_tick,
+                    info);
+}
+
+cave_status cave_ctx_set_timing(cave_ctx* ctx, int enable) {
+    if (!ctx) return CAVE_ERR_INVALID_ARG;
+    CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (enable && !ctx->ev[0]) {
+        for (auto& e : ctx->ev) CAVE_CUDA(ctx, cudaEventCreate(&e));
+    }
+    ctx->timing = enable != 0;
+    return CAVE_OK;
+}
+
+cave_status cave_ctx_last_timing(const cave_ctx* ctx, cave_timing* out) {
+    if (!ctx || !out) return CAVE_ERR_INVALID_ARG;
+    *out = ctx->last_timing;
+    return CAVE_OK;
+}
+
+}  // extern "C"
+
+static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* host_out, const cave_sim_params* params,
+                            const uint64_t* validBitmasks, uint32_t nValid, uint32_t maxRuleBits, uint32_t nticks,
+                            uint32_t maxTicks, cave_tick_stats* per_tick, cave_grid_info* info) {
     if (!g || !params) return CAVE_ERR_INVALID_ARG;
     cave_ctx* ctx = g->ctx;
     DecodedRule d;
     if (!decode_params(*params, validBitmasks, nValid, maxRuleBits, d))
         return set_error(ctx, CAVE_ERR_INVALID_ARG, "rule index outside the valid-bitmask table");
     StreamPlan plan;
-    if (!plan_stream(0, g->X, g->Y, g->Z, (uint32_t)ctx->sm_count * 2, 0, plan))
-        return set_error(ctx, CAVE_ERR_INVALID_ARG, "grid shape not supported by the streaming kernel (X <= 1024, Y,Z <= 65535)");
+    // Tile-shape overrides for tuning sweeps: CAVE_STREAM_ROWS (rows per CTA incl. halo) and
+    // CAVE_STREAM_CTAS_PER_SM (CTAs per tick per SM).
+    const char* env_rows = std::getenv("CAVE_STREAM_ROWS");
+    const char* env_cps = std::getenv("CAVE_STREAM_CTAS_PER_SM");
+    const uint32_t rows_hint = env_rows ? (uint32_t)std::atoi(env_rows) : 0u;
+    const uint32_t cps = env_cps ? std::max(1, std::atoi(env_cps)) : 2u;
+    if (!plan_stream(0, g->X, g->Y, g->Z, (uint32_t)ctx->sm_count * cps, rows_hint, plan))
+        return set_error(ctx, CAVE_ERR_INVALID_ARG,
+                         "grid shape not supported by the streaming kernel (X <= 1024, Y, Z <= 65535)");
     CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
     const uint64_t nstrips = (uint64_t)plan.SX * g->Y * g->Z;
     if (!g->strips) {
@@ -344,29 +419,41 @@ cave_status cave_run(cave_grid* g, const cave_sim_params* params, const uint64_t
         e = cudaMemcpyAsync(ditems, plan.items.data(), sizeof(StreamItem) * plan.items.size(), cudaMemcpyHostToDevice,
                             ctx->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(g->sim, &s, sizeof(s), cudaMemcpyHostToDevice, ctx->stream);
+    record(ctx, 0);
+    if (e == cudaSuccess && host_in)
+        e = cudaMemcpyAsync(g->nib[g->cur], host_in, g->words * 4, cudaMemcpyHostToDevice, ctx->stream);
+    record(ctx, 1);
     if (e == cudaSuccess) e = launch_nib_to_strips(g->nib[g->cur], g->strips, g->X, g->Y, g->Z, ctx->stream);
-    const bool sparse = rule_is_sparse(s.rule);
+    record(ctx, 2);
     for (uint32_t t = 0; t < nticks && e == cudaSuccess; t++)
-        e = launch_stream_tick((int)(d.flags & 7u), sparse, ditems, (uint32_t)plan.items.size(), g->sim, g->strips,
-                               plan.SX, plan.SXp, plan.threads, ctx->stream);
+        e = launch_stream_tick((int)(d.flags & 7u), (int)s.rule.nterms, &s.rule, ditems, (uint32_t)plan.items.size(),
+                               g->sim, g->strips, plan.SX, plan.SXp, plan.threads, ctx->stream);
+    record(ctx, 3);
+    // Raw stepping never stops early, so the result is in copy (nticks & 1).
+    if (e == cudaSuccess)
+        e = launch_strips_to_nib(g->strips + (uint64_t)(nticks & 1u) * nstrips, g->nib[g->cur], g->X, g->Y, g->Z,
+                                 ctx->stream);
+    record(ctx, 4);
+    if (e == cudaSuccess && host_out)
+        e = cudaMemcpyAsync(host_out, g->nib[g->cur], g->words * 4, cudaMemcpyDeviceToHost, ctx->stream);
     StripSim back;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&back, g->sim, sizeof(back), cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    if (e == cudaSuccess) {
-        const uint4* cur = g->strips + (back.tick & 1u) * nstrips;
-        e = launch_strips_to_nib(cur, g->nib[g->cur], g->X, g->Y, g->Z, ctx->stream);
-    }
     if (e == cudaSuccess && per_tick && nticks)
         e = cudaMemcpyAsync(per_tick, dticks, sizeof(cave_tick_stats) * nticks, cudaMemcpyDeviceToHost, ctx->stream);
+    record(ctx, 5);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     cudaFree(dticks);
     cudaFree(ditems);
     if (e != cudaSuccess) return check_cuda(ctx, e, "cave_run");
+    finish_timing(ctx, nticks, nticks + 2, true);
     if (back.error & kErrWaitTimeout) return set_error(ctx, CAVE_ERR_TIMEOUT, "streaming kernel: bulk-copy wait timed out");
     if (back.error) return set_error(ctx, CAVE_ERR_INTERNAL, "streaming kernel raised an error flag");
+    if (back.tick != nticks) return set_error(ctx, CAVE_ERR_INTERNAL, "streaming run stopped early");
     if (info) *info = back.info;
     return CAVE_OK;
 }
+
+extern "C" {
 
 void cave_manager_update(const cave_grid_snapshot* snapshot, cave_grid_info* info, cave_sim_params* perms,
                          uint64_t maxPermutation, uint64_t survivalEndPermutation, uint32_t maxTicks,

@@ -16,6 +16,9 @@ struct cave_ctx {
     int sm_count = 148;
     std::string last_error;
     std::mutex mu;  // guards last_error
+    bool timing = false;
+    cudaEvent_t ev[6] = {};  // created when timing is enabled
+    cave_timing last_timing = {};
 };
 
 struct cave_grid {
@@ -51,7 +54,8 @@ struct StreamPlan {
     std::vector<StreamItem> items;
 };
 // Builds the work items of simulation `sim_index` with grid X*Y*Z; `target_ctas` is the
-// number of CTAs one tick should spread over (a multiple of the SM count).
+// number of CTAs one tick should spread over (a multiple of the SM count); rows_hint = rows
+// per CTA including the two halo rows (0 = default).
 bool plan_stream(uint32_t sim_index, uint32_t X, uint32_t Y, uint32_t Z, uint32_t target_ctas,
                  uint32_t rows_hint, StreamPlan& plan);
 

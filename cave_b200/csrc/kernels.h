@@ -36,8 +36,11 @@ cudaError_t launch_strips_to_nib(const uint4* strips, uint32_t* nib, uint32_t X,
 cudaError_t launch_seed_nib(uint32_t* nib, const SeedSpec& sp, cudaStream_t st);
 cudaError_t launch_seed_strips(uint4* strips, const SeedSpec& sp, cudaStream_t st);
 // threads = rows * SXp (rows includes the two halo rows), SXp = power of two >= SX, <= 32.
-cudaError_t launch_stream_tick(int nb, bool sparse, const StreamItem* items, uint32_t n_items, StripSim* sims,
-                               uint4* pool, uint32_t SX, uint32_t SXp, uint32_t threads, cudaStream_t st);
-size_t stream_smem_bytes_host(uint32_t rows, uint32_t SX, uint32_t SXp);
+// nt: sparse term count of the rule (0 = mux tree). param_rule: the rule of every item's
+// simulation when the launch holds one simulation only (passed as a kernel parameter), else null.
+// Launches use programmatic dependent launch, so consecutive ticks overlap set-up and drain.
+cudaError_t launch_stream_tick(int nb, int nt, const DeviceRule* param_rule, const StreamItem* items,
+                               uint32_t n_items, StripSim* sims, uint4* pool, uint32_t SX, uint32_t SXp,
+                               uint32_t threads, cudaStream_t st);
 
 }  // namespace cave

@@ -48,7 +48,7 @@ DeviceRule make_device_rule(const DecodedRule& d) {
     const int nterms = std::popcount(u);
     const int nbits = count_bits(nb);
     const int tree_cost = 2 * ((1 << nbits) - 1);
-    if (nterms <= kMaxTerms && nterms * 9 < tree_cost) {
+    if (nterms <= kMaxSparseTerms && nterms * 9 < tree_cost) {
         int t = 0;
         for (int k = 0; k < 32; k++) {
             if (!((u >> k) & 1u)) continue;

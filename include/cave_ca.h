@@ -104,6 +104,19 @@ const char* cave_last_error(const cave_ctx* ctx);
 /* Blocks until all work queued on the context's stream is done. */
 cave_status cave_ctx_synchronize(cave_ctx* ctx);
 
+/* Device-side timing of the last cave_step / cave_run call, measured with CUDA events on
+ * the context's stream (replaces the reference's timestamp queries, queryManager.h:13-97).
+ * Recorded only while enabled (off by default; it adds one event pair per phase). */
+typedef struct {
+    uint32_t ticks;          /* tick launches in the call                               */
+    uint32_t launches;       /* kernels this library launched in the call               */
+    float tick_ms;           /* from the first tick launch to the end of the last one   */
+    float convert_ms;        /* layout conversions (nibble <-> bit-plane), both ways    */
+    float total_ms;          /* whole call on the device, copies included               */
+} cave_timing;
+cave_status cave_ctx_set_timing(cave_ctx* ctx, int enable);
+cave_status cave_ctx_last_timing(const cave_ctx* ctx, cave_timing* out);
+
 /* ---- grids --------------------------------------------------------------------------- */
 typedef struct cave_grid cave_grid;
 
@@ -148,6 +161,15 @@ cave_status cave_step(cave_grid* g, const cave_sim_params* params, const uint64_
 cave_status cave_run(cave_grid* g, const cave_sim_params* params, const uint64_t* validBitmasks,
                      uint32_t nValid, uint32_t maxRuleBits, uint32_t nticks, uint32_t maxTicks,
                      cave_tick_stats* per_tick, cave_grid_info* info);
+
+/* cave_run with host buffers: copies in_words (nwords, host memory, ideally pinned) to the
+ * grid, runs, and copies the result to out_words, all in one stream-ordered call -- the
+ * end-to-end form of the reference's upload / tick loop / read-back
+ * (searchSystem.cpp:314, :480-629, :631-644). */
+cave_status cave_run_host(cave_grid* g, const uint32_t* in_words, uint32_t* out_words, uint64_t nwords,
+                          const cave_sim_params* params, const uint64_t* validBitmasks, uint32_t nValid,
+                          uint32_t maxRuleBits, uint32_t nticks, uint32_t maxTicks, cave_tick_stats* per_tick,
+                          cave_grid_info* info);
 
 /* ---- manager (host restatement) ------------------------------------------------------ */
 /* One dispatch of searchManager.slang computeMain (:98-149) including NextPermutation

@@ -136,6 +136,17 @@ def test_wide_rows_1024(ctx):
         check_path(ctx, X, Y, Z, params, init, 3, path)
 
 
+@pytest.mark.parametrize("dims", [(512, 70, 5), (1024, 40, 4), (480, 95, 7)])
+def test_wide_rows_many_tiles(ctx, dims):
+    """Wide rows split into several y-tiles: halo rows are real rows of the neighbouring tile
+    and must be neither double-counted nor read past the exchange buffer."""
+    X, Y, Z = dims
+    rng = np.random.default_rng(X + Y)
+    init = random_states(rng, X, Y, Z, 15)
+    params = O.make_params(15, 7, 0x10, 0x18)
+    check_path(ctx, X, Y, Z, params, init, 4, "run", every_tick=False)
+
+
 # ---------------------------------------------------------------- seeding
 @pytest.mark.parametrize("dims", [(49, 49, 49), (25, 25, 25), (33, 40, 17)])
 @pytest.mark.parametrize("random_fill,density_index,seed,size_index", [(0, 15, 0, 0), (1, 7, 3, 0), (1, 2, 9, 5),
