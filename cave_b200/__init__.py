@@ -63,6 +63,16 @@ class TickStats(ctypes.Structure):
                                            tuple(self.bbox_max))
 
 
+class SimDesc(ctypes.Structure):
+    _fields_ = [("params", SimParams), ("init", u32), ("maxTicks", u32), ("validTable", u32), ("tag", u32)]
+
+
+class SimResult(ctypes.Structure):
+    _fields_ = [("info", GridInfo), ("category", u32), ("tag", u32), ("population", u32), ("activeTicks", u32),
+                ("totalChanged", u64), ("bbox_min", u32 * 3), ("bbox_max", u32 * 3), ("params", SimParams),
+                ("error", u32), ("pad", u32)]
+
+
 class Timing(ctypes.Structure):
     _fields_ = [("ticks", u32), ("launches", u32), ("tick_ms", ctypes.c_float), ("convert_ms", ctypes.c_float),
                 ("total_ms", ctypes.c_float)]
@@ -99,6 +109,16 @@ _SIGS = {
     "cave_manager_update": (None, [P(GridSnapshot), P(GridInfo), P(SimParams), u64, u64, u32, P(GridInfo),
                                    P(SimParams)]),
     "cave_enumerate_valid_bitmasks": (u64, [u32, u32, P(u64), u64]),
+    "cave_batch_create": (i32, [ctypes.c_void_p, P(ctypes.c_void_p)]),
+    "cave_batch_destroy": (None, [ctypes.c_void_p]),
+    "cave_batch_add_init": (i32, [ctypes.c_void_p, u32, u32, u32, P(u32), u64, P(u32)]),
+    "cave_batch_add_init_seeded": (i32, [ctypes.c_void_p, u32, u32, u32, u32, u32, u32, u64, u32, u32, P(u32)]),
+    "cave_batch_add_table": (i32, [ctypes.c_void_p, P(u64), u32, P(u32)]),
+    "cave_batch_add_sims": (i32, [ctypes.c_void_p, P(SimDesc), u64, u32]),
+    "cave_batch_launch": (i32, [ctypes.c_void_p]),
+    "cave_batch_poll": (i32, [ctypes.c_void_p]),
+    "cave_batch_results": (i32, [ctypes.c_void_p, P(SimResult), u64]),
+    "cave_batch_size": (u64, [ctypes.c_void_p]),
 }
 
 
@@ -258,3 +278,64 @@ def manager_update(snapshot: GridSnapshot, info: GridInfo, perms: SimParams, max
     lib().cave_manager_update(ctypes.byref(snapshot), ctypes.byref(info), ctypes.byref(perms), max_permutation,
                               survival_end, max_ticks, ctypes.byref(ic), ctypes.byref(pc))
     return ic, pc
+
+
+class Batch:
+    """Many independent simulations run to completion on the device (cave_batch)."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        h = ctypes.c_void_p()
+        ctx.check(lib().cave_batch_create(ctx.h, ctypes.byref(h)), "cave_batch_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().cave_batch_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def add_init(self, X, Y, Z, words) -> int:
+        w = np.ascontiguousarray(words, dtype=np.uint32)
+        ix = u32()
+        self.ctx.check(lib().cave_batch_add_init(self.h, X, Y, Z, _u32p(w), w.size, ctypes.byref(ix)),
+                       "cave_batch_add_init")
+        return ix.value
+
+    def add_init_seeded(self, X, Y, Z, spawn, threshold, run_seed, max_cell_state) -> int:
+        ix = u32()
+        self.ctx.check(lib().cave_batch_add_init_seeded(self.h, X, Y, Z, spawn[0], spawn[1], spawn[2], threshold,
+                                                        run_seed, max_cell_state, ctypes.byref(ix)),
+                       "cave_batch_add_init_seeded")
+        return ix.value
+
+    def add_table(self, valid) -> int:
+        v = np.ascontiguousarray(valid, dtype=np.uint64)
+        ix = u32()
+        self.ctx.check(lib().cave_batch_add_table(self.h, _u64p(v), v.size, ctypes.byref(ix)), "cave_batch_add_table")
+        return ix.value
+
+    def add_sims(self, descs, max_rule_bits=0):
+        arr = (SimDesc * len(descs))(*descs)
+        self.ctx.check(lib().cave_batch_add_sims(self.h, arr, len(descs), max_rule_bits), "cave_batch_add_sims")
+
+    def launch(self):
+        self.ctx.check(lib().cave_batch_launch(self.h), "cave_batch_launch")
+
+    def poll(self) -> bool:
+        rc = lib().cave_batch_poll(self.h)
+        if rc == ERR_NOT_READY:
+            return False
+        self.ctx.check(rc, "cave_batch_poll")
+        return True
+
+    def results(self):
+        n = lib().cave_batch_size(self.h)
+        out = (SimResult * max(n, 1))()
+        self.ctx.check(lib().cave_batch_results(self.h, out, n), "cave_batch_results")
+        return [out[i] for i in range(n)]

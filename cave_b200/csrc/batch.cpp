@@ -1,0 +1,340 @@
+// batch.cpp -- cave_batch_*: many independent simulations in persistent device launches.
+//
+// Replaces the chunk / slot machinery of SearchSystem (searchSystem.cpp:126-394, :480-713):
+// instead of one dispatch per slot per tick plus a host fence per tick, every simulation of
+// the batch is queued on the device and run to completion (status > 0) by the resident
+// kernel, one launch per (grid shape, neighbourhood, rule-evaluation) class.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <tuple>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/cave_ca.h"
+#include "context.h"
+#include "kernels.h"
+#include "rules.h"
+
+namespace cave {
+
+struct InitGrid {
+    uint32_t X, Y, Z;
+    uint64_t offset;  // in strips, into the batch's pool
+};
+
+struct PendingSim {
+    cave_sim_desc d;
+    uint32_t maxRuleBits;
+};
+
+struct RuleKey {
+    uint32_t maxcs, flags;
+    uint64_t birth, survival;
+    bool operator==(const RuleKey& o) const {
+        return maxcs == o.maxcs && flags == o.flags && birth == o.birth && survival == o.survival;
+    }
+};
+struct RuleKeyHash {
+    size_t operator()(const RuleKey& k) const noexcept {
+        size_t h = std::hash<uint64_t>{}(k.birth * 0x9E3779B97F4A7C15ull ^ k.survival);
+        return h ^ (std::hash<uint32_t>{}(k.maxcs * 31u + k.flags) << 1);
+    }
+};
+
+// Largest resident grid: strips * 16 B plus the exchange buffers must fit in shared memory.
+constexpr size_t kMaxResidentSmem = 220 * 1024;
+
+bool resident_fits(uint32_t X, uint32_t Y, uint32_t Z) {
+    const uint32_t SX = (X + 31u) / 32u;
+    uint32_t SXp = 1;
+    while (SXp < SX) SXp <<= 1;
+    if (SX > 32 || (uint64_t)Y * SXp > 1024) return false;
+    return resident_smem_bytes(X, Y, Z, 1) <= kMaxResidentSmem;
+}
+
+// Launch geometry of one resident class: segments of ~8-12 planes, <= 1024 threads.
+ResLaunch resident_geometry(uint32_t X, uint32_t Y, uint32_t Z, uint32_t& threads) {
+    ResLaunch P{};
+    P.X = X;
+    P.Y = Y;
+    P.Z = Z;
+    P.SX = (X + 31u) / 32u;
+    uint32_t SXp = 1, lg = 0;
+    while (SXp < P.SX) {
+        SXp <<= 1;
+        lg++;
+    }
+    P.sxp_log2 = lg;
+    const uint32_t cols = Y * SXp;
+    uint32_t nseg = std::max(1u, std::min<uint32_t>(1024u / cols, (Z + 7u) / 8u));
+    while (nseg > 1 && resident_smem_bytes(X, Y, Z, nseg) > kMaxResidentSmem) nseg--;
+    P.nseg = nseg;
+    P.seg_len = (Z + nseg - 1) / nseg;
+    threads = (nseg * cols + 31u) / 32u * 32u;
+    return P;
+}
+
+}  // namespace cave
+
+using namespace cave;
+
+struct cave_batch {
+    cave_ctx* ctx = nullptr;
+    uint4* pool = nullptr;
+    uint64_t pool_cap = 0, pool_used = 0;  // strips
+    std::vector<InitGrid> inits;
+    std::vector<std::vector<uint64_t>> tables;
+    std::vector<PendingSim> sims;
+    // launch state
+    DeviceRule* d_rules = nullptr;
+    ResSim* d_sims = nullptr;
+    cave_sim_result* d_results = nullptr;
+    uint32_t* d_queues = nullptr;
+    std::vector<cave_sim_params> translated;
+    cudaEvent_t done = nullptr;
+    bool launched = false;
+    uint64_t launched_n = 0;
+};
+
+static cave_status reserve_pool(cave_batch* b, uint64_t strips) {
+    cave_ctx* ctx = b->ctx;
+    if (b->pool_used + strips <= b->pool_cap) return CAVE_OK;
+    const uint64_t cap = std::max<uint64_t>({b->pool_cap * 2, b->pool_used + strips, 1u << 16});
+    uint4* np = nullptr;
+    CAVE_CUDA(ctx, cudaMalloc(&np, cap * 16));
+    if (b->pool_used)
+        CAVE_CUDA(ctx, cudaMemcpyAsync(np, b->pool, b->pool_used * 16, cudaMemcpyDeviceToDevice, ctx->stream));
+    CAVE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    cudaFree(b->pool);
+    b->pool = np;
+    b->pool_cap = cap;
+    return CAVE_OK;
+}
+
+static void free_launch(cave_batch* b) {
+    cudaFree(b->d_rules);
+    cudaFree(b->d_sims);
+    cudaFree(b->d_results);
+    cudaFree(b->d_queues);
+    b->d_rules = nullptr;
+    b->d_sims = nullptr;
+    b->d_results = nullptr;
+    b->d_queues = nullptr;
+}
+
+extern "C" {
+
+cave_status cave_batch_create(cave_ctx* ctx, cave_batch** out) {
+    if (!ctx || !out) return CAVE_ERR_INVALID_ARG;
+    *out = nullptr;
+    CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
+    cave_batch* b = new (std::nothrow) cave_batch();
+    if (!b) return CAVE_ERR_OUT_OF_MEMORY;
+    b->ctx = ctx;
+    if (cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess) {
+        delete b;
+        return CAVE_ERR_CUDA;
+    }
+    *out = b;
+    return CAVE_OK;
+}
+
+void cave_batch_destroy(cave_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->ctx->device);
+    cudaStreamSynchronize(b->ctx->stream);
+    free_launch(b);
+    cudaFree(b->pool);
+    cudaEventDestroy(b->done);
+    delete b;
+}
+
+uint64_t cave_batch_size(const cave_batch* b) { return b ? b->sims.size() : 0; }
+
+cave_status cave_batch_add_init(cave_batch* b, uint32_t X, uint32_t Y, uint32_t Z, const uint32_t* words,
+                                uint64_t nwords, uint32_t* index) {
+    if (!b || !words || !index || X == 0 || Y == 0 || Z == 0 || nwords != cave_grid_words(X, Y, Z))
+        return CAVE_ERR_INVALID_ARG;
+    cave_ctx* ctx = b->ctx;
+    CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
+    const uint64_t strips = (uint64_t)((X + 31) / 32) * Y * Z;
+    cave_status rc = reserve_pool(b, strips);
+    if (rc) return rc;
+    uint32_t* tmp = nullptr;
+    CAVE_CUDA(ctx, cudaMalloc(&tmp, nwords * 4));
+    cudaError_t e = cudaMemcpyAsync(tmp, words, nwords * 4, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = launch_nib_to_strips(tmp, b->pool + b->pool_used, X, Y, Z, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(tmp);
+    if (e != cudaSuccess) return check_cuda(ctx, e, "cave_batch_add_init");
+    *index = (uint32_t)b->inits.size();
+    b->inits.push_back(InitGrid{X, Y, Z, b->pool_used});
+    b->pool_used += strips;
+    return CAVE_OK;
+}
+
+cave_status cave_batch_add_init_seeded(cave_batch* b, uint32_t X, uint32_t Y, uint32_t Z, uint32_t spawnX,
+                                       uint32_t spawnY, uint32_t spawnZ, uint64_t threshold, uint32_t runSeedIndex,
+                                       uint32_t maxCellState, uint32_t* index) {
+    if (!b || !index || X == 0 || Y == 0 || Z == 0 || threshold > (1ull << 32)) return CAVE_ERR_INVALID_ARG;
+    cave_ctx* ctx = b->ctx;
+    CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
+    const uint64_t strips = (uint64_t)((X + 31) / 32) * Y * Z;
+    cave_status rc = reserve_pool(b, strips);
+    if (rc) return rc;
+    SeedSpec sp = make_seed_spec(X, Y, Z, spawnX, spawnY, spawnZ, 0, threshold, threshold == (1ull << 32),
+                                 runSeedIndex, maxCellState);
+    CAVE_CUDA(ctx, launch_seed_strips(b->pool + b->pool_used, sp, ctx->stream));
+    *index = (uint32_t)b->inits.size();
+    b->inits.push_back(InitGrid{X, Y, Z, b->pool_used});
+    b->pool_used += strips;
+    return CAVE_OK;
+}
+
+cave_status cave_batch_add_table(cave_batch* b, const uint64_t* validBitmasks, uint32_t nValid, uint32_t* index) {
+    if (!b || !index || (nValid && !validBitmasks)) return CAVE_ERR_INVALID_ARG;
+    *index = (uint32_t)b->tables.size();
+    b->tables.emplace_back(validBitmasks, validBitmasks + nValid);
+    return CAVE_OK;
+}
+
+cave_status cave_batch_add_sims(cave_batch* b, const cave_sim_desc* sims, uint64_t n, uint32_t maxRuleBits) {
+    if (!b || (n && !sims)) return CAVE_ERR_INVALID_ARG;
+    if (b->launched) return set_error(b->ctx, CAVE_ERR_INVALID_ARG, "batch already launched");
+    for (uint64_t i = 0; i < n; i++) {
+        if (sims[i].init >= b->inits.size())
+            return set_error(b->ctx, CAVE_ERR_INVALID_ARG, "simulation refers to an unknown initial grid");
+        if (maxRuleBits > 0 && sims[i].validTable >= b->tables.size())
+            return set_error(b->ctx, CAVE_ERR_INVALID_ARG, "simulation refers to an unknown K-index table");
+    }
+    b->sims.reserve(b->sims.size() + n);
+    for (uint64_t i = 0; i < n; i++) b->sims.push_back(PendingSim{sims[i], maxRuleBits});
+    return CAVE_OK;
+}
+
+cave_status cave_batch_launch(cave_batch* b) {
+    if (!b) return CAVE_ERR_INVALID_ARG;
+    cave_ctx* ctx = b->ctx;
+    if (b->launched) return set_error(ctx, CAVE_ERR_INVALID_ARG, "batch already launched");
+    CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
+    const uint64_t n = b->sims.size();
+    // rules: decode, translate K-indices, deduplicate
+    std::vector<DeviceRule> rules;
+    std::unordered_map<RuleKey, uint32_t, RuleKeyHash> rule_ix;
+    std::vector<uint32_t> sim_rule(n);
+    b->translated.resize(n);
+    for (uint64_t i = 0; i < n; i++) {
+        const PendingSim& ps = b->sims[i];
+        const std::vector<uint64_t>* tab = ps.maxRuleBits ? &b->tables[ps.d.validTable] : nullptr;
+        DecodedRule d;
+        if (!decode_params(ps.d.params, tab ? tab->data() : nullptr, tab ? (uint32_t)tab->size() : 0, ps.maxRuleBits, d))
+            return set_error(ctx, CAVE_ERR_INVALID_ARG, "rule index outside the valid-bitmask table");
+        cave_sim_params tp = ps.d.params;
+        if (ps.maxRuleBits) {  // searchSystem.cpp:676-684
+            tp.birthAndMaxCellStateRules = (tp.birthAndMaxCellStateRules & ~kPermMask) | d.birth;
+            tp.survivalAndNeighborhoodRules = (tp.survivalAndNeighborhoodRules & ~kPermMask) | d.survival;
+        }
+        b->translated[i] = tp;
+        RuleKey k{d.maxcs, d.flags & 7u, d.birth, d.survival};
+        auto it = rule_ix.find(k);
+        if (it == rule_ix.end()) {
+            it = rule_ix.emplace(k, (uint32_t)rules.size()).first;
+            rules.push_back(make_device_rule(d));
+        }
+        sim_rule[i] = it->second;
+    }
+    // classes: (grid shape, neighbourhood, term count)
+    using ClassKey = std::tuple<uint32_t, uint32_t, uint32_t, uint32_t, uint32_t>;
+    std::map<ClassKey, std::vector<uint32_t>> classes;
+    for (uint64_t i = 0; i < n; i++) {
+        const InitGrid& g = b->inits[b->sims[i].d.init];
+        if (!resident_fits(g.X, g.Y, g.Z))
+            return set_error(ctx, CAVE_ERR_INVALID_ARG,
+                             "batched simulation grid too large for shared memory (use cave_run per grid)");
+        const DeviceRule& r = rules[sim_rule[i]];
+        classes[ClassKey{g.X, g.Y, g.Z, r.flags & 7u, r.nterms}].push_back((uint32_t)i);
+    }
+    std::vector<ResSim> rs;
+    rs.reserve(n);
+    struct Launch {
+        ResLaunch P;
+        uint32_t nb, nt, threads, first;
+    };
+    std::vector<Launch> launches;
+    for (auto& [key, idx] : classes) {
+        Launch L{};
+        uint32_t threads = 0;
+        L.P = resident_geometry(std::get<0>(key), std::get<1>(key), std::get<2>(key), threads);
+        L.P.n_sims = (uint32_t)idx.size();
+        L.nb = std::get<3>(key);
+        L.nt = std::get<4>(key);
+        L.threads = threads;
+        L.first = (uint32_t)rs.size();
+        for (uint32_t i : idx) {
+            const PendingSim& ps = b->sims[i];
+            rs.push_back(ResSim{sim_rule[i], (uint32_t)b->inits[ps.d.init].offset, ps.d.maxTicks, i});
+        }
+        launches.push_back(L);
+    }
+    free_launch(b);
+    cudaError_t e = cudaSuccess;
+    if (n) {
+        e = cudaMalloc(&b->d_rules, sizeof(DeviceRule) * std::max<size_t>(rules.size(), 1));
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_sims, sizeof(ResSim) * n);
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_results, sizeof(cave_sim_result) * n);
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_queues, sizeof(uint32_t) * launches.size());
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(b->d_rules, rules.data(), sizeof(DeviceRule) * rules.size(), cudaMemcpyHostToDevice,
+                                ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(b->d_sims, rs.data(), sizeof(ResSim) * n, cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(b->d_queues, 0, sizeof(uint32_t) * launches.size(), ctx->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(b->d_results, 0, sizeof(cave_sim_result) * n, ctx->stream);
+    }
+    for (size_t li = 0; li < launches.size() && e == cudaSuccess; li++) {
+        const Launch& L = launches[li];
+        const size_t smem = resident_smem_bytes(L.P.X, L.P.Y, L.P.Z, L.P.nseg);
+        // resident CTAs per SM: bounded by shared memory (228 KB per SM, 1 KB reserved per CTA)
+        const uint32_t per_sm = std::max<uint32_t>(1u, (uint32_t)((228u * 1024u) / (smem + 3 * 1024u)));
+        const uint32_t by_threads = std::max<uint32_t>(1u, 2048u / L.threads);
+        const uint32_t ctas = std::min<uint64_t>((uint64_t)ctx->sm_count * std::min(per_sm, by_threads), L.P.n_sims);
+        e = launch_resident((int)L.nb, (int)L.nt, L.P, b->d_sims + L.first, b->d_rules, b->pool, b->d_results,
+                            b->d_queues + li, ctas, L.threads, ctx->stream);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(b->done, ctx->stream);
+    if (e != cudaSuccess) return check_cuda(ctx, e, "cave_batch_launch");
+    b->launched = true;
+    b->launched_n = n;
+    return CAVE_OK;
+}
+
+cave_status cave_batch_poll(cave_batch* b) {
+    if (!b || !b->launched) return CAVE_ERR_INVALID_ARG;
+    const cudaError_t e = cudaEventQuery(b->done);
+    if (e == cudaErrorNotReady) return CAVE_ERR_NOT_READY;
+    if (e != cudaSuccess) return check_cuda(b->ctx, e, "cave_batch_poll");
+    return CAVE_OK;
+}
+
+cave_status cave_batch_results(cave_batch* b, cave_sim_result* out, uint64_t n) {
+    if (!b || !b->launched || (n && !out) || n > b->launched_n) return CAVE_ERR_INVALID_ARG;
+    cave_ctx* ctx = b->ctx;
+    CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
+    CAVE_CUDA(ctx, cudaEventSynchronize(b->done));
+    if (n) CAVE_CUDA(ctx, cudaMemcpy(out, b->d_results, sizeof(cave_sim_result) * n, cudaMemcpyDeviceToHost));
+    bool err = false;
+    for (uint64_t i = 0; i < n; i++) {
+        out[i].tag = b->sims[i].d.tag;
+        out[i].params = b->translated[i];
+        err |= out[i].error != 0;
+    }
+    if (err) return set_error(ctx, CAVE_ERR_TIMEOUT, "a batched simulation raised a device error flag");
+    return CAVE_OK;
+}
+
+}  // extern "C"

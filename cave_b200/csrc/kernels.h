@@ -35,6 +35,25 @@ cudaError_t launch_strips_to_nib(const uint4* strips, uint32_t* nib, uint32_t X,
                                  cudaStream_t st);
 cudaError_t launch_seed_nib(uint32_t* nib, const SeedSpec& sp, cudaStream_t st);
 cudaError_t launch_seed_strips(uint4* strips, const SeedSpec& sp, cudaStream_t st);
+// ---- resident batched kernel
+struct ResLaunch {           // geometry shared by every simulation of one launch
+    uint32_t X, Y, Z, SX;
+    uint32_t sxp_log2;       // lanes per row = 1 << sxp_log2 >= SX
+    uint32_t nseg, seg_len;  // z-segments per CTA and planes per segment
+    uint32_t n_sims;
+};
+struct ResSim {              // one simulation of a resident launch
+    uint32_t rule;           // index into the DeviceRule table
+    uint32_t init;           // offset (in strips) of the initial grid in the initial-grid pool
+    uint32_t max_ticks;
+    uint32_t result;         // index into the result array
+};
+size_t resident_smem_bytes(uint32_t X, uint32_t Y, uint32_t Z, uint32_t nseg);
+// nt: sparse term count of every rule in the launch (0 = mux tree), nb: neighbourhood bits.
+cudaError_t launch_resident(int nb, int nt, const ResLaunch& P, const ResSim* sims, const DeviceRule* rules,
+                            const uint4* inits, cave_sim_result* results, uint32_t* queue, uint32_t ctas,
+                            uint32_t threads, cudaStream_t st);
+
 // threads = rows * SXp (rows includes the two halo rows), SXp = power of two >= SX, <= 32.
 // nt: sparse term count of the rule (0 = mux tree). param_rule: the rule of every item's
 // simulation when the launch holds one simulation only (passed as a kernel parameter), else null.

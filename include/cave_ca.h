@@ -171,6 +171,62 @@ cave_status cave_run_host(cave_grid* g, const uint32_t* in_words, uint32_t* out_
                           uint32_t maxRuleBits, uint32_t nticks, uint32_t maxTicks, cave_tick_stats* per_tick,
                           cave_grid_info* info);
 
+/* ---- batched path: many small simulations ------------------------------------------ */
+/* One simulation of a batch: a rule run from an initial grid until the search manager
+ * reports status > 0 (early death, or maxTicks reached), exactly the per-rule lifecycle of a
+ * SearchSystem slot (searchSystem.cpp:496-526, :608-616; searchManager.slang:98-149). */
+typedef struct {
+    cave_sim_params params;   /* rule; K-index form when maxRuleBits > 0 */
+    uint32_t init;            /* index of the initial grid (cave_batch_add_init)        */
+    uint32_t maxTicks;        /* MAX_NUMBER_OF_TICKS_TO_SURVIVE                          */
+    uint32_t validTable;      /* index of the K-index table (cave_batch_add_table)      */
+    uint32_t tag;             /* caller's id, copied to the result                       */
+} cave_sim_desc;
+
+/* Result of one simulation: the final GridInfo plus the derived statistics. */
+typedef struct {
+    cave_grid_info info;      /* as the manager's copy buffer at the final tick          */
+    uint32_t category;        /* 0 viable, 1 possible, 2 unviable (searchSystem.cpp:697-711) */
+    uint32_t tag;
+    uint32_t population;      /* non-zero cells after the final tick                     */
+    uint32_t activeTicks;     /* ticks in which at least one cell changed                */
+    uint64_t totalChanged;    /* cells changed, summed over ticks                        */
+    uint32_t bbox_min[3];     /* of the non-zero cells after the final tick              */
+    uint32_t bbox_max[3];
+    cave_sim_params params;   /* rule with K-indices translated to bitmasks (:668-685)   */
+    uint32_t error;
+    uint32_t pad;
+} cave_sim_result;
+
+typedef struct cave_batch cave_batch;
+
+/* A batch owns device copies of initial grids, K-index tables and simulation descriptors.
+ * Replaces the chunk-level buffers and the per-slot tick loop of SearchSystem
+ * (searchSystem.cpp:126-394, :480-713) by one persistent launch per simulation class. */
+cave_status cave_batch_create(cave_ctx* ctx, cave_batch** out);
+void cave_batch_destroy(cave_batch* b);
+/* Adds an initial grid in the reference nibble layout (host words). Returns its index. */
+cave_status cave_batch_add_init(cave_batch* b, uint32_t X, uint32_t Y, uint32_t Z, const uint32_t* words,
+                                uint64_t nwords, uint32_t* index);
+/* Adds an initial grid seeded on the device (searchSystem.cpp:219-306 with an explicit fill
+ * threshold, as cave_grid_seed_threshold). Returns its index. */
+cave_status cave_batch_add_init_seeded(cave_batch* b, uint32_t X, uint32_t Y, uint32_t Z, uint32_t spawnX,
+                                       uint32_t spawnY, uint32_t spawnZ, uint64_t threshold,
+                                       uint32_t runSeedIndex, uint32_t maxCellState, uint32_t* index);
+/* Adds a K-index table (EnumerateValidBitmasks order). Returns its index. */
+cave_status cave_batch_add_table(cave_batch* b, const uint64_t* validBitmasks, uint32_t nValid, uint32_t* index);
+/* Queues simulations (maxRuleBits applies to all of them). */
+cave_status cave_batch_add_sims(cave_batch* b, const cave_sim_desc* sims, uint64_t n, uint32_t maxRuleBits);
+/* Starts every queued simulation on the device (non-blocking). */
+cave_status cave_batch_launch(cave_batch* b);
+/* Non-blocking completion poll (the IsTickComplete of searchSystem.cpp:467-478): CAVE_OK
+ * when the launched work has finished, CAVE_ERR_NOT_READY otherwise. */
+cave_status cave_batch_poll(cave_batch* b);
+/* Waits for the launched work and copies results (in queue order) to out[0..n). */
+cave_status cave_batch_results(cave_batch* b, cave_sim_result* out, uint64_t n);
+/* Simulations queued so far. */
+uint64_t cave_batch_size(const cave_batch* b);
+
 /* ---- manager (host restatement) ------------------------------------------------------ */
 /* One dispatch of searchManager.slang computeMain (:98-149) including NextPermutation
  * (:56-96), for callers that drive the plain path themselves. */
