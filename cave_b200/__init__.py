@@ -73,6 +73,56 @@ class SimResult(ctypes.Structure):
                 ("error", u32), ("pad", u32)]
 
 
+class SearchConfig(ctypes.Structure):
+    _fields_ = [("grid", u32), ("gridSweepMin", u32), ("gridSweepMax", u32), ("gridSweepStep", u32),
+                ("spawnX", u32), ("spawnY", u32), ("spawnZ", u32), ("spawnMode", u32),
+                ("spawnDensity", ctypes.c_float), ("densitySweepMin", ctypes.c_float),
+                ("densitySweepMax", ctypes.c_float), ("densitySweepStep", ctypes.c_float), ("seedRuns", u32),
+                ("faces", u32), ("edges", u32), ("corners", u32), ("wrap", u32), ("minMaxCellState", u32),
+                ("maxMaxCellState", u32), ("maxTicks", u32), ("maxRuleBits", u32), ("chunksPerConfig", u32),
+                ("outputFolder", ctypes.c_char_p)]
+
+
+class SearchSummary(ctypes.Structure):
+    _fields_ = [("sims", u64), ("viable", u64), ("possible", u64), ("unviable", u64), ("ticks", u64),
+                ("cellUpdates", u64), ("chunks", u32), ("uniqueRules", u32), ("deviceSeconds", ctypes.c_double),
+                ("wallSeconds", ctypes.c_double)]
+
+
+def search_config(grid=49, spawn=11, spawn_mode="filled", density=0.5, neighborhood="F", min_cs=3, max_cs=10,
+                  ticks=50, max_rule_bits=0, chunks_per_config=1, seed_runs=1, grid_sweep=None, density_sweep=None,
+                  output=None) -> SearchConfig:
+    """SearchConfig from the reference CLI's search flags (defaults as src/main.cpp:29-44, except
+    --chunks-per-config, whose partitions only change scheduling)."""
+    c = SearchConfig()
+    c.grid = grid
+    if grid_sweep:
+        c.gridSweepMin, c.gridSweepMax, c.gridSweepStep = grid_sweep
+    c.spawnX = c.spawnY = c.spawnZ = spawn
+    c.spawnMode = 0 if spawn_mode == "random" else 1
+    c.spawnDensity = density
+    if density_sweep:
+        c.densitySweepMin, c.densitySweepMax, c.densitySweepStep = density_sweep
+    c.seedRuns = seed_runs
+    c.faces, c.edges, c.corners, c.wrap = [int(ch in neighborhood) for ch in "FECW"]
+    c.minMaxCellState, c.maxMaxCellState = min_cs, max_cs
+    c.maxTicks = ticks
+    c.maxRuleBits = max_rule_bits
+    c.chunksPerConfig = chunks_per_config
+    c.outputFolder = (output.encode() if output else None)
+    return c
+
+
+def rule_string_to_bitmask(s: str) -> int:
+    return int(lib().cave_rule_string_to_bitmask(s.encode()))
+
+
+def bitmask_to_rule_string(mask: int) -> str:
+    buf = ctypes.create_string_buffer(512)
+    lib().cave_bitmask_to_rule_string(mask, buf, 512)
+    return buf.value.decode()
+
+
 class Timing(ctypes.Structure):
     _fields_ = [("ticks", u32), ("launches", u32), ("tick_ms", ctypes.c_float), ("convert_ms", ctypes.c_float),
                 ("total_ms", ctypes.c_float)]
@@ -119,6 +169,10 @@ _SIGS = {
     "cave_batch_poll": (i32, [ctypes.c_void_p]),
     "cave_batch_results": (i32, [ctypes.c_void_p, P(SimResult), u64]),
     "cave_batch_size": (u64, [ctypes.c_void_p]),
+    "cave_batch_run_plain": (i32, [ctypes.c_void_p, u32, P(ctypes.c_double)]),
+    "cave_search_run": (i32, [ctypes.c_void_p, P(SearchConfig), u32, u64, P(SearchSummary)]),
+    "cave_rule_string_to_bitmask": (u64, [ctypes.c_char_p]),
+    "cave_bitmask_to_rule_string": (u64, [u64, ctypes.c_char_p, u64]),
 }
 
 
@@ -272,6 +326,14 @@ class Grid:
         return ([pt[i] for i in range(nticks)] if stats else None), info
 
 
+def search_run(ctx: Context, config: SearchConfig, plain=False, sim_limit=0) -> SearchSummary:
+    """A whole search sweep (cave_search_run); mode plain = the per-slot per-tick path."""
+    s = SearchSummary()
+    ctx.check(lib().cave_search_run(ctx.h, ctypes.byref(config), 1 if plain else 0, sim_limit, ctypes.byref(s)),
+              "cave_search_run")
+    return s
+
+
 def manager_update(snapshot: GridSnapshot, info: GridInfo, perms: SimParams, max_permutation, survival_end,
                    max_ticks):
     ic, pc = GridInfo(), SimParams()
@@ -326,6 +388,12 @@ class Batch:
 
     def launch(self):
         self.ctx.check(lib().cave_batch_launch(self.h), "cave_batch_launch")
+
+    def run_plain(self, slots) -> float:
+        """Plain path (one launch per slot per tick); returns device seconds."""
+        s = ctypes.c_double()
+        self.ctx.check(lib().cave_batch_run_plain(self.h, slots, ctypes.byref(s)), "cave_batch_run_plain")
+        return s.value
 
     def poll(self) -> bool:
         rc = lib().cave_batch_poll(self.h)

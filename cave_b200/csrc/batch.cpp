@@ -99,6 +99,8 @@ struct cave_batch {
     cudaEvent_t done = nullptr;
     bool launched = false;
     uint64_t launched_n = 0;
+    bool plain = false;                      // results came from cave_batch_run_plain
+    std::vector<cave_sim_result> host_results;
 };
 
 static cave_status reserve_pool(cave_batch* b, uint64_t strips) {
@@ -325,8 +327,12 @@ cave_status cave_batch_results(cave_batch* b, cave_sim_result* out, uint64_t n) 
     if (!b || !b->launched || (n && !out) || n > b->launched_n) return CAVE_ERR_INVALID_ARG;
     cave_ctx* ctx = b->ctx;
     CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
-    CAVE_CUDA(ctx, cudaEventSynchronize(b->done));
-    if (n) CAVE_CUDA(ctx, cudaMemcpy(out, b->d_results, sizeof(cave_sim_result) * n, cudaMemcpyDeviceToHost));
+    if (b->plain) {
+        std::memcpy(out, b->host_results.data(), sizeof(cave_sim_result) * n);
+    } else {
+        CAVE_CUDA(ctx, cudaEventSynchronize(b->done));
+        if (n) CAVE_CUDA(ctx, cudaMemcpy(out, b->d_results, sizeof(cave_sim_result) * n, cudaMemcpyDeviceToHost));
+    }
     bool err = false;
     for (uint64_t i = 0; i < n; i++) {
         out[i].tag = b->sims[i].d.tag;
@@ -334,6 +340,159 @@ cave_status cave_batch_results(cave_batch* b, cave_sim_result* out, uint64_t n) 
         err |= out[i].error != 0;
     }
     if (err) return set_error(ctx, CAVE_ERR_TIMEOUT, "a batched simulation raised a device error flag");
+    return CAVE_OK;
+}
+
+cave_status cave_batch_run_plain(cave_batch* b, uint32_t nslots, double* deviceSeconds) {
+    if (!b || nslots == 0) return CAVE_ERR_INVALID_ARG;
+    cave_ctx* ctx = b->ctx;
+    if (b->launched) return set_error(ctx, CAVE_ERR_INVALID_ARG, "batch already launched");
+    CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
+    const uint64_t n = b->sims.size();
+    // K-index tables, concatenated
+    std::vector<uint64_t> tabs;
+    std::vector<uint64_t> tab_off(b->tables.size());
+    for (size_t t = 0; t < b->tables.size(); t++) {
+        tab_off[t] = tabs.size();
+        tabs.insert(tabs.end(), b->tables[t].begin(), b->tables[t].end());
+    }
+    // validate rules and translate K-indices (searchSystem.cpp:676-684)
+    b->translated.resize(n);
+    for (uint64_t i = 0; i < n; i++) {
+        const PendingSim& ps = b->sims[i];
+        const std::vector<uint64_t>* tab = ps.maxRuleBits ? &b->tables[ps.d.validTable] : nullptr;
+        DecodedRule d;
+        if (!decode_params(ps.d.params, tab ? tab->data() : nullptr, tab ? (uint32_t)tab->size() : 0, ps.maxRuleBits, d))
+            return set_error(ctx, CAVE_ERR_INVALID_ARG, "rule index outside the valid-bitmask table");
+        cave_sim_params tp = ps.d.params;
+        if (ps.maxRuleBits) {
+            tp.birthAndMaxCellStateRules = (tp.birthAndMaxCellStateRules & ~kPermMask) | d.birth;
+            tp.survivalAndNeighborhoodRules = (tp.survivalAndNeighborhoodRules & ~kPermMask) | d.survival;
+        }
+        b->translated[i] = tp;
+    }
+    // initial grids in the nibble layout, converted once from the strip pool
+    std::vector<uint64_t> init_off(b->inits.size());
+    uint64_t init_words = 0, max_words = 0;
+    for (size_t i = 0; i < b->inits.size(); i++) {
+        init_off[i] = init_words;
+        const uint64_t w = cave_grid_words(b->inits[i].X, b->inits[i].Y, b->inits[i].Z);
+        init_words += w;
+        max_words = std::max(max_words, w);
+    }
+    nslots = (uint32_t)std::min<uint64_t>(nslots, std::max<uint64_t>(n, 1));
+    uint32_t *d_init = nullptr, *d_cells = nullptr;
+    uint64_t* d_tabs = nullptr;
+    PlainSlot* d_slots = nullptr;
+    struct Free {
+        std::vector<void*> p;
+        ~Free() {
+            for (void* q : p) cudaFree(q);
+        }
+    } fr;
+    CAVE_CUDA(ctx, cudaMalloc(&d_init, std::max<uint64_t>(init_words, 1) * 4));
+    fr.p.push_back(d_init);
+    CAVE_CUDA(ctx, cudaMalloc(&d_cells, std::max<uint64_t>(max_words, 1) * 4 * 2 * nslots));
+    fr.p.push_back(d_cells);
+    CAVE_CUDA(ctx, cudaMalloc(&d_tabs, std::max<size_t>(tabs.size(), 1) * 8));
+    fr.p.push_back(d_tabs);
+    CAVE_CUDA(ctx, cudaMalloc(&d_slots, sizeof(PlainSlot) * nslots));
+    fr.p.push_back(d_slots);
+    if (!tabs.empty()) CAVE_CUDA(ctx, cudaMemcpy(d_tabs, tabs.data(), tabs.size() * 8, cudaMemcpyHostToDevice));
+    for (size_t i = 0; i < b->inits.size(); i++)
+        CAVE_CUDA(ctx, launch_strips_to_nib(b->pool + b->inits[i].offset, d_init + init_off[i], b->inits[i].X,
+                                            b->inits[i].Y, b->inits[i].Z, ctx->stream));
+    b->host_results.assign(n, cave_sim_result{});
+    std::vector<PlainSlot> hs(nslots);
+    std::vector<int64_t> sim_of(nslots, -1);  // simulation in each slot
+    std::vector<int> cur(nslots, 0);
+    std::vector<uint64_t> changed(nslots, 0);
+    std::vector<uint32_t> active(nslots, 0);
+    uint64_t next = 0, done = 0;
+    cudaEvent_t e0, e1;
+    CAVE_CUDA(ctx, cudaEventCreate(&e0));
+    CAVE_CUDA(ctx, cudaEventCreate(&e1));
+    double dev_ms = 0;
+    cudaError_t e = cudaSuccess;
+    auto start_sim = [&](uint32_t s) {
+        const uint64_t i = next++;
+        sim_of[s] = (int64_t)i;
+        const PendingSim& ps = b->sims[i];
+        const InitGrid& g = b->inits[ps.d.init];
+        const uint64_t words = cave_grid_words(g.X, g.Y, g.Z);
+        cur[s] = 0;
+        changed[s] = 0;
+        active[s] = 0;
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_cells + (uint64_t)s * 2 * max_words, d_init + init_off[ps.d.init], words * 4,
+                                cudaMemcpyDeviceToDevice, ctx->stream);
+        PlainSlot& p = hs[s];
+        std::memset(&p, 0, sizeof(p));
+        for (int k = 0; k < 3; k++) p.bmin[k] = 0xFFFFFFFFu;
+        p.perms = ps.d.params;
+        p.permsCopy = ps.d.params;
+        p.run_manager = 1;
+        p.maxTicks = ps.d.maxTicks;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d_slots + s, &p, sizeof(p), cudaMemcpyHostToDevice, ctx->stream);
+    };
+    for (uint32_t s = 0; s < nslots && next < n; s++) start_sim(s);
+    while (done < n && e == cudaSuccess) {
+        cudaEventRecord(e0, ctx->stream);
+        for (uint32_t s = 0; s < nslots && e == cudaSuccess; s++) {
+            if (sim_of[s] < 0) continue;
+            const PendingSim& ps = b->sims[(uint64_t)sim_of[s]];
+            const InitGrid& g = b->inits[ps.d.init];
+            uint32_t* base = d_cells + (uint64_t)s * 2 * max_words;
+            const uint64_t words = cave_grid_words(g.X, g.Y, g.Z);
+            const std::vector<uint64_t>* tab = ps.maxRuleBits ? &b->tables[ps.d.validTable] : nullptr;
+            e = launch_plain_step(base + (uint64_t)cur[s] * words, base + (uint64_t)(cur[s] ^ 1) * words, g.X, g.Y, g.Z,
+                                  d_slots + s, tab ? d_tabs + tab_off[ps.d.validTable] : nullptr,
+                                  tab ? (uint32_t)tab->size() : 0u, ps.maxRuleBits, ctx->stream);
+            cur[s] ^= 1;
+        }
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(hs.data(), d_slots, sizeof(PlainSlot) * nslots, cudaMemcpyDeviceToHost, ctx->stream);
+        cudaEventRecord(e1, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);  // the tick fence
+        if (e != cudaSuccess) break;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        dev_ms += ms;
+        for (uint32_t s = 0; s < nslots; s++) {
+            if (sim_of[s] < 0) continue;
+            const PlainSlot& p = hs[s];
+            if (p.error) {
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                return set_error(ctx, CAVE_ERR_INVALID_ARG, "plain step raised an error flag");
+            }
+            changed[s] += p.last.changed;
+            if (p.last.changed) active[s]++;
+            if (p.infoCopy.status == 0) continue;
+            const uint64_t i = (uint64_t)sim_of[s];
+            cave_sim_result& r = b->host_results[i];
+            r.info = p.infoCopy;
+            const uint64_t mcs = ((b->sims[i].d.params.birthAndMaxCellStateRules >> 60) & 0xF) + 1;
+            r.category = r.info.status == 2 ? 0u : ((uint64_t)r.info.numberOfSimulationTicksSurvived > mcs + 1 ? 1u : 2u);
+            r.population = p.last.population;
+            r.activeTicks = active[s];
+            r.totalChanged = changed[s];
+            for (int k = 0; k < 3; k++) {
+                r.bbox_min[k] = p.last.bbox_min[k];
+                r.bbox_max[k] = p.last.bbox_max[k];
+            }
+            done++;
+            sim_of[s] = -1;
+            if (next < n) start_sim(s);
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return check_cuda(ctx, e, "cave_batch_run_plain");
+    if (deviceSeconds) *deviceSeconds = dev_ms / 1e3;
+    b->plain = true;
+    b->launched = true;
+    b->launched_n = n;
     return CAVE_OK;
 }
 

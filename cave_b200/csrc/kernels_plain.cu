@@ -39,13 +39,17 @@ __global__ void __launch_bounds__(256) k_plain_step(PlainArgs A) {
     const uint32_t maxCS = (uint32_t)(P.birthAndMaxCellStateRules >> 60) + 1u;
     const uint32_t flags = (uint32_t)(P.survivalAndNeighborhoodRules >> 60);
     uint64_t B, S;
-    bool bad = false;
+    bool bad = false, skip = false;
     if (A.maxRuleBits > 0) {
+        // An exhausted slot (NULL permutation) is still dispatched for one tick after its last
+        // rule, as in searchSystem.cpp:541-564; its K-indices are meaningless and the manager
+        // ignores its snapshot (searchManager.slang:104-110), so nothing is computed.
+        skip = P.birthAndMaxCellStateRules == 0 || P.survivalAndNeighborhoodRules == 0;
         const uint32_t bi = (uint32_t)(P.birthAndMaxCellStateRules & kPermMask) - 1u;
         const uint32_t si = (uint32_t)(P.survivalAndNeighborhoodRules & kPermMask) - 1u;
-        bad = (bi >= A.nValid || si >= A.nValid);
-        B = bad ? 0 : A.valid[bi];
-        S = bad ? 0 : A.valid[si];
+        bad = !skip && (bi >= A.nValid || si >= A.nValid);
+        B = (bad || skip) ? 0 : A.valid[bi];
+        S = (bad || skip) ? 0 : A.valid[si];
     } else {
         B = P.birthAndMaxCellStateRules & kPermMask;
         S = P.survivalAndNeighborhoodRules & kPermMask;
@@ -55,7 +59,7 @@ __global__ void __launch_bounds__(256) k_plain_step(PlainArgs A) {
     uint32_t died = 0, dying = 0, born = 0, surv = 0, pop = 0;
     uint32_t bmin[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, bmax[3] = {0, 0, 0};
 
-    if (idx < nwords && !bad) {
+    if (idx < nwords && !bad && !skip) {
         const uint32_t ux = (uint32_t)(idx % A.W);
         const uint64_t r = idx / A.W;
         const uint32_t y = (uint32_t)(r % A.Y);

@@ -1,0 +1,556 @@
+// search.cpp -- cave_search_run: the reference's search mode on top of the CUDA paths.
+//
+// Sweep expansion follows searchMode.cpp:49-218, per-chunk slot set-up searchSystem.cpp:34-200,
+// classification searchSystem.cpp:646-713, JSONL lines searchSystem.cpp:959-978, file names
+// searchMode.cpp:104-120 and :1030-1038, aggregation ruleAggregator.h:19-141.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <filesystem>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/cave_ca.h"
+#include "context.h"
+#include "kernels.h"
+#include "rules.h"
+
+namespace cave {
+
+struct GridConfig {          // SearchGridConfig (searchSystem.h:20-26)
+    uint32_t maxCellState;
+    uint32_t flags;          // neighbourhood bits incl. W
+    uint64_t maxPermutation; // 2^n - 1, or the K-index table size when K > 0
+    uint32_t neighborCount;
+    std::vector<uint64_t> valid;  // K-index table (K > 0)
+};
+
+struct Chunk {               // ChunkConfiguration (structs.h:109-128)
+    uint32_t X, Y, Z;
+    uint32_t spawnX, spawnY, spawnZ;
+    uint32_t spawnRegionShapeId;
+    uint32_t densityIndex, seed;
+    uint32_t partitionIndex, partitionCount;
+    uint32_t ordinal;
+};
+
+struct SimRef {              // one (chunk, slot, survival, birth) simulation
+    uint32_t chunk, slot;
+    uint64_t survival, birth;  // 1-based indices (K > 0) or raw masks (K == 0)
+};
+
+struct Outcome {
+    cave_sim_params params;  // translated rule
+    cave_grid_info info;
+    uint32_t category;
+};
+
+static uint32_t density_index(float p) {  // searchMode.cpp:135-136, :175
+    int i = (int)(p * 16.0f) - 1;
+    return (uint32_t)std::clamp(i, 0, 15);
+}
+
+static uint64_t threshold_from_index(uint32_t idx) {  // searchSystem.cpp:240, :260-262
+    const float d = ((float)idx + 1.0f) / 16.0f;
+    if (d >= 1.0f) return 1ull << 32;
+    return (uint64_t)(uint32_t)(d * 4294967296.0);
+}
+
+struct Sweep {
+    std::vector<GridConfig> configs;
+    std::vector<Chunk> chunks;
+    std::string folder, prefixBase;
+};
+
+static Sweep expand(const cave_search_config& c) {
+    Sweep s;
+    // neighbourhood subsets (searchMode.cpp:50-69)
+    std::vector<uint32_t> nbs;
+    uint32_t sel = (c.faces ? 1u : 0u) | (c.edges ? 2u : 0u) | (c.corners ? 4u : 0u);
+    for (uint32_t sub = 1; sub <= sel; sub++) {
+        if ((sub & sel) == sub) {
+            nbs.push_back(sub);
+            if (c.wrap) nbs.push_back(sub | 8u);
+        }
+    }
+    if (nbs.empty()) nbs.push_back(1u);
+    // grid configs (searchMode.cpp:81-102) and K-index tables (searchSystem.cpp:38-53)
+    for (uint32_t m = c.minMaxCellState; m <= c.maxMaxCellState; m++) {
+        for (uint32_t f : nbs) {
+            GridConfig g;
+            g.maxCellState = m;
+            g.flags = f;
+            g.neighborCount = neighbor_count(f);
+            g.maxPermutation = g.neighborCount < 60 ? ((1ull << g.neighborCount) - 1) : kPermMask;
+            if (c.maxRuleBits > 0) {
+                g.valid = enumerate_valid_bitmasks(g.neighborCount, c.maxRuleBits);
+                g.maxPermutation = g.valid.size();
+            }
+            s.configs.push_back(std::move(g));
+        }
+    }
+    // file prefix (searchMode.cpp:104-120)
+    std::string tag;
+    if (c.faces) tag += "F";
+    if (c.edges) tag += "E";
+    if (c.corners) tag += "C";
+    if (c.wrap) tag += "W";
+    if (tag.empty()) tag = "F";
+    s.prefixBase = "cs" + std::to_string(c.minMaxCellState) + "-" + std::to_string(c.maxMaxCellState) + "_" + tag +
+                   "_t" + std::to_string(c.maxTicks);
+    if (c.maxRuleBits > 0) s.prefixBase += "_b" + std::to_string(c.maxRuleBits);
+    if (c.outputFolder && *c.outputFolder) s.folder = std::string(c.outputFolder) + "cube/";
+    // chunk axes (searchMode.cpp:143-218)
+    std::vector<uint32_t> grids;
+    if (c.gridSweepStep > 0 && c.gridSweepMin > 0 && c.gridSweepMin <= c.gridSweepMax) {
+        for (uint32_t g = c.gridSweepMin; g <= c.gridSweepMax; g += c.gridSweepStep) grids.push_back(g);
+    } else {
+        grids.push_back(c.grid);
+    }
+    std::vector<uint32_t> dens;
+    if (c.densitySweepStep > 0.0f && c.spawnMode == 0 && c.densitySweepMin <= c.densitySweepMax) {
+        for (float d = c.densitySweepMin; d <= c.densitySweepMax + 1e-6f; d += c.densitySweepStep)
+            dens.push_back(density_index(d));
+    } else {
+        dens.push_back(density_index(c.spawnDensity));
+    }
+    const uint32_t seeds = std::max(1u, c.seedRuns);
+    const uint32_t parts = std::max(1u, c.chunksPerConfig);
+    uint32_t ordinal = 1;
+    for (uint32_t g : grids) {
+        const uint32_t X = g, Y = g, Z = g;
+        for (uint32_t d : dens)
+            for (uint32_t sd = 0; sd < seeds; sd++)
+                for (uint32_t p = 0; p < parts; p++) {
+                    Chunk ch{};
+                    ch.X = X;
+                    ch.Y = Y;
+                    ch.Z = Z;
+                    ch.spawnX = std::min(c.spawnX, X);
+                    ch.spawnY = std::min(c.spawnY, Y);
+                    ch.spawnZ = std::min(c.spawnZ, Z);
+                    ch.spawnRegionShapeId = c.spawnMode;
+                    ch.densityIndex = d;
+                    ch.seed = sd;
+                    ch.partitionIndex = p;
+                    ch.partitionCount = parts;
+                    ch.ordinal = ordinal++;
+                    s.chunks.push_back(ch);
+                }
+    }
+    return s;
+}
+
+// Survival range of a slot in a chunk (searchSystem.cpp:88-96, :170-188); empty when degenerate.
+static void survival_range(const GridConfig& g, const Chunk& ch, uint64_t& lo, uint64_t& hi) {
+    hi = g.maxPermutation;
+    lo = 1;
+    if (ch.partitionCount > 1) {
+        hi = (uint64_t)(ch.partitionIndex + 1) * g.maxPermutation / ch.partitionCount;
+        lo = 1 + (uint64_t)ch.partitionIndex * g.maxPermutation / ch.partitionCount;
+    }
+}
+
+static std::string chunk_prefix(const Sweep& s, const Chunk& ch) {  // searchMode.cpp:1030-1038, :1078
+    return s.prefixBase + "_c" + std::to_string(ch.ordinal) + "_g" + std::to_string(ch.X) + "x" +
+           std::to_string(ch.Y) + "x" + std::to_string(ch.Z) + "_d" + std::to_string(ch.densityIndex) + "_s" +
+           std::to_string(ch.seed) + "_gpu0";
+}
+
+// nlohmann::json dump() of the entry at searchSystem.cpp:964-976: keys sorted, compact.
+static std::string result_line(const Outcome& o) {
+    char buf[512];
+    std::snprintf(buf, sizeof(buf),
+                  "{\"birthAndMaxCellStateRules\":%llu,\"finalAliveCount\":%u,\"maxAliveCount\":%u,"
+                  "\"shapeAndGridConfiguration\":%llu,\"survivalAndNeighborhoodRules\":%llu,\"ticksSurvived\":%u,"
+                  "\"totalBirths\":%u,\"totalDeaths\":%u}",
+                  (unsigned long long)o.params.birthAndMaxCellStateRules, o.info.finalAliveCount,
+                  o.info.maxAliveCount, (unsigned long long)o.params.shapeAndGridConfiguration,
+                  (unsigned long long)o.params.survivalAndNeighborhoodRules, o.info.numberOfSimulationTicksSurvived,
+                  o.info.totalNumberOfCellsThatWereBorn, o.info.totalNumberOfCellsThatDied);
+    return buf;
+}
+
+struct AggStats {  // RuleStats (ruleAggregator.h:57-66)
+    uint32_t total = 0, viable = 0, possible = 0, unviable = 0, maxT = 0, minT = UINT32_MAX;
+    uint64_t sumT = 0;
+};
+using AggKey = std::tuple<uint64_t, uint64_t, uint32_t, uint32_t, uint32_t>;  // birth, survival, maxCS, flags, shape
+
+static void aggregate(std::map<AggKey, AggStats>& agg, const Outcome& o) {  // ruleAggregator.h:69-90
+    AggKey k{o.params.birthAndMaxCellStateRules & kPermMask, o.params.survivalAndNeighborhoodRules & kPermMask,
+             (uint32_t)((o.params.birthAndMaxCellStateRules >> 60) & 0xF) + 1,
+             (uint32_t)(o.params.survivalAndNeighborhoodRules >> 60), 0u};
+    AggStats& st = agg[k];
+    st.total++;
+    if (o.category == 0) st.viable++;
+    else if (o.category == 1) st.possible++;
+    else st.unviable++;
+    const uint32_t t = o.info.numberOfSimulationTicksSurvived;
+    st.maxT = std::max(st.maxT, t);
+    st.minT = std::min(st.minT, t);
+    st.sumT += t;
+}
+
+static bool write_aggregate(const std::string& path, const std::map<AggKey, AggStats>& agg) {  // :105-135
+    std::ofstream out(path, std::ios::out | std::ios::trunc);
+    if (!out.is_open()) return false;
+    for (const auto& [k, st] : agg) {
+        const float avg = st.total ? (float)st.sumT / (float)st.total : 0.0f;
+        const float rate = st.total ? (float)st.viable / (float)st.total : 0.0f;
+        out << "{\"birth\":" << std::get<0>(k) << ",\"survival\":" << std::get<1>(k)
+            << ",\"maxCellState\":" << std::get<2>(k) << ",\"neighborhoodFlags\":" << std::get<3>(k)
+            << ",\"shapeId\":" << std::get<4>(k) << ",\"totalRuns\":" << st.total << ",\"viableRuns\":" << st.viable
+            << ",\"possibleRuns\":" << st.possible << ",\"unviableRuns\":" << st.unviable
+            << ",\"viabilityRate\":" << rate << ",\"minTicksSurvived\":" << (st.minT == UINT32_MAX ? 0 : st.minT)
+            << ",\"maxTicksSurvived\":" << st.maxT << ",\"avgTicksSurvived\":" << avg << "}\n";
+    }
+    return out.good();
+}
+
+// ---------------------------------------------------------------- batched execution
+static cave_status run_batched(cave_ctx* ctx, const cave_search_config& c, const Sweep& s,
+                               std::vector<std::vector<Outcome>>& per_chunk, uint64_t limit, double& dev_s,
+                               uint64_t& nsims) {
+    cave_batch* b = nullptr;
+    cave_status rc = cave_batch_create(ctx, &b);
+    if (rc) return rc;
+    struct Guard {
+        cave_batch* b;
+        ~Guard() { cave_batch_destroy(b); }
+    } guard{b};
+    // K-index tables, one per grid config
+    std::vector<uint32_t> table_ix(s.configs.size(), 0);
+    if (c.maxRuleBits > 0)
+        for (size_t i = 0; i < s.configs.size(); i++) {
+            rc = cave_batch_add_table(b, s.configs[i].valid.data(), (uint32_t)s.configs[i].valid.size(), &table_ix[i]);
+            if (rc) return rc;
+        }
+    std::vector<cave_sim_desc> descs;
+    std::vector<std::pair<uint32_t, uint32_t>> owner;  // (chunk, position)
+    for (uint32_t ci = 0; ci < s.chunks.size(); ci++) {
+        const Chunk& ch = s.chunks[ci];
+        // initial cells per maxCellState (searchSystem.cpp:219-306): one grid per distinct maxCS
+        std::map<uint32_t, uint32_t> init_ix;
+        const bool random = ch.spawnRegionShapeId == 0;
+        const uint64_t thr = random ? threshold_from_index(ch.densityIndex) : (1ull << 32);
+        for (size_t gi = 0; gi < s.configs.size(); gi++) {
+            const uint32_t m = s.configs[gi].maxCellState;
+            if (init_ix.count(m)) continue;
+            uint32_t ix = 0;
+            rc = cave_batch_add_init_seeded(b, ch.X, ch.Y, ch.Z, ch.spawnX, ch.spawnY, ch.spawnZ, thr, ch.seed, m, &ix);
+            if (rc) return rc;
+            init_ix[m] = ix;
+        }
+        for (uint32_t gi = 0; gi < s.configs.size(); gi++) {
+            const GridConfig& g = s.configs[gi];
+            uint64_t lo, hi;
+            survival_range(g, ch, lo, hi);
+            for (uint64_t sv = lo; sv <= hi; sv++)
+                for (uint64_t bi = 1; bi <= g.maxPermutation; bi++) {  // birth index fastest
+                    if (limit && descs.size() >= limit) break;
+                    cave_sim_desc d{};
+                    d.params.birthAndMaxCellStateRules = ((uint64_t)((g.maxCellState - 1) & 0xF) << 60) | bi;
+                    d.params.survivalAndNeighborhoodRules = ((uint64_t)(g.flags & 0xF) << 60) | sv;
+                    d.params.shapeAndGridConfiguration = 0;
+                    d.init = init_ix[g.maxCellState];
+                    d.maxTicks = c.maxTicks;
+                    d.validTable = table_ix[gi];
+                    d.tag = (uint32_t)descs.size();
+                    owner.emplace_back(ci, gi);
+                    descs.push_back(d);
+                }
+        }
+    }
+    rc = cave_batch_add_sims(b, descs.data(), descs.size(), c.maxRuleBits);
+    if (rc) return rc;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, ctx->stream);
+    rc = cave_batch_launch(b);
+    cudaEventRecord(e1, ctx->stream);
+    if (rc) return rc;
+    std::vector<cave_sim_result> res(descs.size());
+    rc = cave_batch_results(b, res.data(), res.size());
+    float ms = 0;
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    dev_s = ms / 1e3;
+    nsims = descs.size();
+    per_chunk.assign(s.chunks.size(), {});
+    for (size_t i = 0; i < res.size(); i++)
+        per_chunk[owner[i].first].push_back(Outcome{res[i].params, res[i].info, res[i].category});
+    return CAVE_OK;
+}
+
+// ---------------------------------------------------------------- plain execution
+// SearchSystem's loop (searchSystem.cpp:480-713): per tick, reset finished slots from their
+// initial cells, launch the step (with the fused manager) once per slot, fence, read the copy
+// buffers and record finished rules.
+static cave_status run_plain(cave_ctx* ctx, const cave_search_config& c, const Sweep& s,
+                             std::vector<std::vector<Outcome>>& per_chunk, uint64_t limit, double& dev_s,
+                             uint64_t& nsims) {
+    per_chunk.assign(s.chunks.size(), {});
+    nsims = 0;
+    double dev_ms = 0;
+    cudaEvent_t e0, e1;
+    CAVE_CUDA(ctx, cudaEventCreate(&e0));
+    CAVE_CUDA(ctx, cudaEventCreate(&e1));
+    for (uint32_t ci = 0; ci < s.chunks.size() && !(limit && nsims >= limit); ci++) {
+        const Chunk& ch = s.chunks[ci];
+        const uint32_t nslot = (uint32_t)s.configs.size();
+        const uint64_t words = cave_grid_words(ch.X, ch.Y, ch.Z);
+        // device buffers: per slot cur/next/initial cells, the slot records, K-index tables
+        uint32_t* cells = nullptr;
+        PlainSlot* slots = nullptr;
+        uint64_t* tables = nullptr;
+        std::vector<uint64_t> tab_off(nslot, 0);
+        std::vector<uint64_t> host_tab;
+        for (uint32_t gi = 0; gi < nslot; gi++) {
+            tab_off[gi] = host_tab.size();
+            host_tab.insert(host_tab.end(), s.configs[gi].valid.begin(), s.configs[gi].valid.end());
+        }
+        CAVE_CUDA(ctx, cudaMalloc(&cells, words * 4 * 3 * nslot));
+        CAVE_CUDA(ctx, cudaMalloc(&slots, sizeof(PlainSlot) * nslot));
+        CAVE_CUDA(ctx, cudaMalloc(&tables, sizeof(uint64_t) * std::max<size_t>(host_tab.size(), 1)));
+        if (!host_tab.empty())
+            CAVE_CUDA(ctx, cudaMemcpy(tables, host_tab.data(), sizeof(uint64_t) * host_tab.size(), cudaMemcpyHostToDevice));
+        std::vector<PlainSlot> hs(nslot);
+        std::vector<int> cur(nslot, 0);
+        const bool random = ch.spawnRegionShapeId == 0;
+        const uint64_t thr = random ? threshold_from_index(ch.densityIndex) : (1ull << 32);
+        for (uint32_t gi = 0; gi < nslot; gi++) {
+            const GridConfig& g = s.configs[gi];
+            uint32_t* base = cells + (uint64_t)gi * 3 * words;
+            SeedSpec sp = make_seed_spec(ch.X, ch.Y, ch.Z, ch.spawnX, ch.spawnY, ch.spawnZ, 0, thr, thr == (1ull << 32),
+                                         ch.seed, g.maxCellState);
+            CAVE_CUDA(ctx, launch_seed_nib(base + 2 * words, sp, ctx->stream));
+            CAVE_CUDA(ctx, cudaMemcpyAsync(base, base + 2 * words, words * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+            PlainSlot& p = hs[gi];
+            std::memset(&p, 0, sizeof(p));
+            for (int k = 0; k < 3; k++) p.bmin[k] = 0xFFFFFFFFu;
+            uint64_t lo, hi;
+            survival_range(g, ch, lo, hi);
+            if (lo <= hi) {  // degenerate partitions start exhausted (searchSystem.cpp:175-188)
+                p.perms.birthAndMaxCellStateRules = ((uint64_t)((g.maxCellState - 1) & 0xF) << 60) | 1;
+                p.perms.survivalAndNeighborhoodRules = ((uint64_t)(g.flags & 0xF) << 60) | lo;
+            }
+            p.permsCopy = p.perms;
+            p.run_manager = 1;
+            p.maxPermutation = g.maxPermutation;
+            p.survivalEnd = hi;
+            p.maxTicks = c.maxTicks;
+        }
+        CAVE_CUDA(ctx, cudaMemcpyAsync(slots, hs.data(), sizeof(PlainSlot) * nslot, cudaMemcpyHostToDevice, ctx->stream));
+        std::vector<cave_sim_params> last_saved(nslot, cave_sim_params{0, 0, 0});
+        std::vector<bool> need_reset(nslot, false);
+        std::vector<cave_sim_params> read_perms(nslot);
+        for (uint32_t gi = 0; gi < nslot; gi++) read_perms[gi] = hs[gi].perms;
+        bool running = true;
+        while (running && !(limit && nsims >= limit)) {
+            cudaEventRecord(e0, ctx->stream);
+            for (uint32_t gi = 0; gi < nslot; gi++) {
+                const bool exhausted = read_perms[gi].birthAndMaxCellStateRules == 0 &&
+                                       read_perms[gi].survivalAndNeighborhoodRules == 0;
+                if (exhausted) continue;  // the reference still dispatches; its result is never read
+                uint32_t* base = cells + (uint64_t)gi * 3 * words;
+                if (need_reset[gi]) {  // Phase 0
+                    CAVE_CUDA(ctx, cudaMemcpyAsync(base + (uint64_t)cur[gi] * words, base + 2 * words, words * 4,
+                                                   cudaMemcpyDeviceToDevice, ctx->stream));
+                    need_reset[gi] = false;
+                }
+                // Phase 1 + 2 (sim + fused manager) + 3 (ping-pong instead of the copy)
+                CAVE_CUDA(ctx, launch_plain_step(base + (uint64_t)cur[gi] * words, base + (uint64_t)(cur[gi] ^ 1) * words,
+                                                 ch.X, ch.Y, ch.Z, slots + gi, c.maxRuleBits ? tables + tab_off[gi] : nullptr,
+                                                 (uint32_t)s.configs[gi].valid.size(), c.maxRuleBits, ctx->stream));
+                cur[gi] ^= 1;
+            }
+            CAVE_CUDA(ctx, cudaMemcpyAsync(hs.data(), slots, sizeof(PlainSlot) * nslot, cudaMemcpyDeviceToHost, ctx->stream));
+            cudaEventRecord(e1, ctx->stream);
+            CAVE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // the tick fence
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            dev_ms += ms;
+            // PollCopyBuffers + CacheCompletedResults (searchSystem.cpp:631-713)
+            running = false;
+            for (uint32_t gi = 0; gi < nslot; gi++) {
+                const cave_grid_info& info = hs[gi].infoCopy;
+                const cave_sim_params& pm = hs[gi].permsCopy;
+                read_perms[gi] = pm;
+                if (pm.birthAndMaxCellStateRules != 0 || pm.survivalAndNeighborhoodRules != 0) running = true;
+                if (hs[gi].error) {
+                    cudaFree(cells);
+                    cudaFree(slots);
+                    cudaFree(tables);
+                    return set_error(ctx, CAVE_ERR_INVALID_ARG, "rule index outside the valid-bitmask table");
+                }
+                if (info.status == 0) continue;
+                if (pm.birthAndMaxCellStateRules == 0 && pm.survivalAndNeighborhoodRules == 0) continue;
+                if (pm.birthAndMaxCellStateRules == last_saved[gi].birthAndMaxCellStateRules &&
+                    pm.survivalAndNeighborhoodRules == last_saved[gi].survivalAndNeighborhoodRules)
+                    continue;
+                last_saved[gi] = pm;
+                need_reset[gi] = true;
+                Outcome o;
+                o.params = pm;
+                if (c.maxRuleBits > 0) {
+                    const auto& v = s.configs[gi].valid;
+                    const uint64_t bi = (pm.birthAndMaxCellStateRules & kPermMask) - 1;
+                    const uint64_t si = (pm.survivalAndNeighborhoodRules & kPermMask) - 1;
+                    if (bi < v.size() && si < v.size()) {
+                        o.params.birthAndMaxCellStateRules = (pm.birthAndMaxCellStateRules & ~kPermMask) | v[bi];
+                        o.params.survivalAndNeighborhoodRules = (pm.survivalAndNeighborhoodRules & ~kPermMask) | v[si];
+                    }
+                }
+                o.info = info;
+                const uint64_t mcs = ((pm.birthAndMaxCellStateRules >> 60) & 0xF) + 1;
+                o.category = info.status == 2 ? 0u : ((uint64_t)info.numberOfSimulationTicksSurvived > mcs + 1 ? 1u : 2u);
+                per_chunk[ci].push_back(o);
+                nsims++;
+            }
+        }
+        cudaFree(cells);
+        cudaFree(slots);
+        cudaFree(tables);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    dev_s = dev_ms / 1e3;
+    return CAVE_OK;
+}
+
+}  // namespace cave
+
+using namespace cave;
+
+extern "C" {
+
+cave_status cave_search_run(cave_ctx* ctx, const cave_search_config* config, uint32_t mode, uint64_t simLimit,
+                            cave_search_summary* summary) {
+    if (!ctx || !config || mode > 1) return CAVE_ERR_INVALID_ARG;
+    const cave_search_config& c = *config;
+    if (c.minMaxCellState < 1 || c.maxMaxCellState > 16 || c.minMaxCellState > c.maxMaxCellState || c.maxTicks == 0)
+        return set_error(ctx, CAVE_ERR_INVALID_ARG, "maxCellState range must lie in 1..16 and ticks must be > 0");
+    const auto t0 = std::chrono::steady_clock::now();
+    CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
+    Sweep s = expand(c);
+    for (const Chunk& ch : s.chunks)
+        if (ch.X == 0 || ch.Y == 0 || ch.Z == 0) return set_error(ctx, CAVE_ERR_INVALID_ARG, "grid extents must be > 0");
+    std::vector<std::vector<Outcome>> per_chunk;
+    double dev_s = 0;
+    uint64_t nsims = 0;
+    cave_status rc = mode == 0 ? run_batched(ctx, c, s, per_chunk, simLimit, dev_s, nsims)
+                               : run_plain(ctx, c, s, per_chunk, simLimit, dev_s, nsims);
+    if (rc) return rc;
+    cave_search_summary sum{};
+    std::map<AggKey, AggStats> agg;
+    if (!s.folder.empty()) {
+        std::error_code ec;
+        std::filesystem::create_directories(s.folder, ec);
+        if (ec) return set_error(ctx, CAVE_ERR_IO, "cannot create " + s.folder);
+    }
+    for (size_t ci = 0; ci < s.chunks.size(); ci++) {
+        const Chunk& ch = s.chunks[ci];
+        std::ofstream f[3];
+        if (!s.folder.empty()) {
+            const std::string p = s.folder + chunk_prefix(s, ch);
+            const char* names[3] = {"_viable.jsonl", "_possible.jsonl", "_unviable.jsonl"};
+            for (int k = 0; k < 3; k++) {
+                f[k].open(p + names[k], std::ios::out | std::ios::trunc);
+                if (!f[k].is_open()) return set_error(ctx, CAVE_ERR_IO, "cannot write " + p + names[k]);
+            }
+        }
+        for (const Outcome& o : per_chunk[ci]) {
+            sum.sims++;
+            (o.category == 0 ? sum.viable : o.category == 1 ? sum.possible : sum.unviable)++;
+            sum.ticks += o.info.numberOfSimulationTicksSurvived;
+            sum.cellUpdates += (uint64_t)o.info.numberOfSimulationTicksSurvived * ch.X * ch.Y * ch.Z;
+            aggregate(agg, o);
+            if (!s.folder.empty()) f[o.category] << result_line(o) << '\n';
+        }
+        for (auto& ff : f)
+            if (ff.is_open() && !ff.good()) return set_error(ctx, CAVE_ERR_IO, "JSONL write failed");
+    }
+    if (!s.folder.empty() && !write_aggregate(s.folder + s.prefixBase + "_aggregate.jsonl", agg))
+        return set_error(ctx, CAVE_ERR_IO, "aggregate JSONL write failed");
+    sum.chunks = (uint32_t)s.chunks.size();
+    sum.uniqueRules = (uint32_t)agg.size();
+    sum.deviceSeconds = dev_s;
+    sum.wallSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    (void)nsims;
+    if (summary) *summary = sum;
+    return CAVE_OK;
+}
+
+// guiSystem.cpp:129-163
+uint64_t cave_rule_string_to_bitmask(const char* rule) {
+    if (!rule) return 0;
+    uint64_t mask = 0;
+    std::stringstream ss(rule);
+    std::string tok;
+    while (std::getline(ss, tok, ',')) {
+        tok.erase(std::remove_if(tok.begin(), tok.end(), [](unsigned char ch) { return std::isspace(ch); }), tok.end());
+        if (tok.empty()) continue;
+        try {
+            const size_t dash = tok.find('-');
+            if (dash != std::string::npos) {
+                const int a = std::stoi(tok.substr(0, dash)), b = std::stoi(tok.substr(dash + 1));
+                for (int i = a; i <= b && i <= 60; i++)
+                    if (i >= 1) mask |= 1ull << (i - 1);
+            } else {
+                const int v = std::stoi(tok);
+                if (v >= 1 && v <= 60) mask |= 1ull << (v - 1);
+            }
+        } catch (...) {
+            // the reference's std::stoi would throw; a malformed token contributes nothing here
+        }
+    }
+    return mask;
+}
+
+// guiSystem.cpp:92-127
+uint64_t cave_bitmask_to_rule_string(uint64_t bitmask, char* out, uint64_t cap) {
+    std::vector<int> bits;
+    for (int b = 0; b < 60; b++)
+        if ((bitmask >> b) & 1) bits.push_back(b + 1);
+    std::string s;
+    if (bits.empty()) {
+        s = "-";
+    } else {
+        size_t i = 0;
+        while (i < bits.size()) {
+            const size_t start = i;
+            while (i + 1 < bits.size() && bits[i + 1] == bits[i] + 1) i++;
+            if (!s.empty()) s += ",";
+            if (i - start >= 2) {
+                s += std::to_string(bits[start]) + "-" + std::to_string(bits[i]);
+            } else {
+                for (size_t j = start; j <= i; j++) {
+                    if (j > start) s += ",";
+                    s += std::to_string(bits[j]);
+                }
+            }
+            i++;
+        }
+    }
+    if (out && cap) {
+        const size_t n = std::min<size_t>(s.size(), cap - 1);
+        std::memcpy(out, s.data(), n);
+        out[n] = '\0';
+    }
+    return s.size();
+}
+
+}  // extern "C"

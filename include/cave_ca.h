@@ -226,6 +226,61 @@ cave_status cave_batch_poll(cave_batch* b);
 cave_status cave_batch_results(cave_batch* b, cave_sim_result* out, uint64_t n);
 /* Simulations queued so far. */
 uint64_t cave_batch_size(const cave_batch* b);
+/* Runs the queued simulations on the plain path instead, the way SearchSystem drives its
+ * slots (searchSystem.cpp:480-713): `slots` simulations in flight, each tick one step launch
+ * per active slot (searchSimulationCube + fused manager), then one read-back and a host fence;
+ * a slot whose rule finished takes the next simulation and restarts from its initial cells.
+ * Blocking. Results are identical to cave_batch_launch's; *deviceSeconds (may be NULL)
+ * receives the device time of the tick loops. */
+cave_status cave_batch_run_plain(cave_batch* b, uint32_t slots, double* deviceSeconds);
+
+/* ---- search sweeps (SearchMode + SearchSystem + RuleAggregator) ------------------------ */
+/* The search flags of the reference CLI (src/main.cpp:27-44, startupConfig.h) that shape a
+ * sweep. A zero step disables a sweep axis. */
+typedef struct {
+    uint32_t grid;                                /* --grid: chunks are grid^3 (searchMode.cpp:160, :218) */
+    uint32_t gridSweepMin, gridSweepMax, gridSweepStep; /* --grid-sweep min:max:step       */
+    uint32_t spawnX, spawnY, spawnZ;              /* --spawn                              */
+    uint32_t spawnMode;                           /* --spawn-mode: 0 random, 1 filled     */
+    float spawnDensity;                           /* --spawn-density                      */
+    float densitySweepMin, densitySweepMax, densitySweepStep; /* --density-sweep           */
+    uint32_t seedRuns;                            /* --seed-runs                          */
+    uint32_t faces, edges, corners, wrap;         /* --neighborhood F/E/C/W               */
+    uint32_t minMaxCellState, maxMaxCellState;    /* --min-cs, --max-cs-range             */
+    uint32_t maxTicks;                            /* --ticks                              */
+    uint32_t maxRuleBits;                         /* --max-rule-bits                      */
+    uint32_t chunksPerConfig;                     /* --chunks-per-config                  */
+    const char* outputFolder;                     /* --output (NULL or "" = no files)     */
+} cave_search_config;
+
+typedef struct {
+    uint64_t sims;           /* (rule, chunk) simulations run                          */
+    uint64_t viable, possible, unviable;
+    uint64_t ticks;          /* ticks run, summed over simulations                    */
+    uint64_t cellUpdates;    /* ticks x grid volume, summed                           */
+    uint32_t chunks;
+    uint32_t uniqueRules;    /* entries of the aggregate                              */
+    double deviceSeconds;    /* device time of the simulation work (CUDA events)      */
+    double wallSeconds;      /* whole call                                            */
+} cave_search_summary;
+
+/* Runs a whole sweep as SearchMode::OnFrame does (searchMode.cpp:49-218 expansion,
+ * :252-459 run, :1030-1054 files and aggregation) and writes, when outputFolder is set,
+ * <out>cube/<prefix>_c<n>_g<X>x<Y>x<Z>_d<d>_s<s>_gpu0_{viable,possible,unviable}.jsonl per chunk
+ * (searchSystem.cpp:959-978 line format, keys sorted) and <out>cube/<prefix>_aggregate.jsonl
+ * (ruleAggregator.h:105-134). mode 0 runs every simulation to completion on the device in
+ * persistent batched launches; mode 1 is the plain path, SearchSystem's own loop -- one
+ * launch per slot per tick and a host fence per tick (searchSystem.cpp:480-713).
+ * simLimit > 0 stops after that many simulations (for sampling the plain path). Lines within
+ * a file are in rule order (slot, survival, birth); the reference writes them in completion
+ * order, which depends on scheduling. */
+cave_status cave_search_run(cave_ctx* ctx, const cave_search_config* config, uint32_t mode, uint64_t simLimit,
+                            cave_search_summary* summary);
+
+/* Reference rule-string helpers (guiSystem.cpp:92-163): "3,5-7" <-> bitmask (bit n-1 = n). */
+uint64_t cave_rule_string_to_bitmask(const char* rule);
+/* Writes the string form of a bitmask into out (capacity cap incl. NUL); returns its length. */
+uint64_t cave_bitmask_to_rule_string(uint64_t bitmask, char* out, uint64_t cap);
 
 /* ---- manager (host restatement) ------------------------------------------------------ */
 /* One dispatch of searchManager.slang computeMain (:98-149) including NextPermutation
