@@ -33,6 +33,7 @@ WORKLOADS = {
     "large512": (512, 1000),
     "large256": (256, 1000),
     "large1024": (1024, 200),
+    "sweep49": (49, 20),
 }
 
 
@@ -290,6 +291,118 @@ def large_workload(args, world, rank, local, pg):
     return line
 
 
+def sweep_descs(G, seeds, cs_values, rank=0, world=1, stride=1):
+    """The config-3 sweep: FE neighbourhood, every survive/birth set with <= 2 bits (171 each),
+    C in cs_values (maxCellState = C - 1), `seeds` seeds; sims of this rank's shard."""
+    import numpy as np
+
+    import cave_b200 as cb
+
+    n_masks = 171
+    per = n_masks * n_masks
+    idx = np.arange(per, dtype=np.int64)
+    si, bi = idx // n_masks, idx % n_masks
+    parts = []
+    init_ix = 0
+    for c in cs_values:
+        mcs = c - 1
+        for s in range(seeds):
+            d = np.zeros(per, dtype=cb.SIM_DESC_DTYPE)
+            d["birth"] = (np.uint64((mcs - 1) & 0xF) << np.uint64(60)) | (bi + 1).astype(np.uint64)
+            d["survival"] = (np.uint64(3) << np.uint64(60)) | (si + 1).astype(np.uint64)
+            d["init"] = init_ix
+            d["maxTicks"] = 20
+            parts.append(d)
+            init_ix += 1
+    allv = np.concatenate(parts)
+    allv["tag"] = np.arange(allv.size, dtype=np.uint32)
+    mine = allv[rank::world]
+    return np.ascontiguousarray(mine[::stride])
+
+
+def sweep_workload(args, world, rank, local, pg):
+    import numpy as np
+
+    import cave_b200 as cb
+    import oracle as O
+
+    G, T = WORKLOADS["sweep49"]
+    seeds, cs_values = 32, (2, 3, 4, 5)
+    thr = O.threshold_from_float(0.30)
+    ctx = cb.Context(local)
+    ctx.set_timing(True)
+    vb = cb.valid_bitmasks(18, 2)
+
+    def make_batch():
+        b = cb.Batch(ctx)
+        for c in cs_values:
+            for s in range(seeds):
+                b.add_init_seeded(G, G, G, (16, 16, 16), thr, s, c - 1)
+        b.add_table(vb)
+        return b
+
+    full = sweep_descs(G, seeds, cs_values, rank, world)
+    warm = np.ascontiguousarray(full[::32])
+    for _ in range(args.warmup):
+        with make_batch() as b:
+            b.add_sims_array(warm, max_rule_bits=2)
+            b.launch()
+            b.results_array()
+    barrier(pg, local)
+    kern_ms, tot_ms, wall, cats, ticks = [], [], [], None, 0
+    for _ in range(args.steps):
+        with make_batch() as b:
+            t0 = time.perf_counter()
+            b.add_sims_array(full, max_rule_bits=2)
+            b.launch()
+            res = b.results_array()
+            wall.append(time.perf_counter() - t0)
+            t = ctx.last_timing()
+            kern_ms.append(t.tick_ms)
+            tot_ms.append(t.total_ms)
+        cats = np.bincount(res["category"], minlength=3)
+        ticks = int(res["info"][:, 2].sum())
+    barrier(pg, local)
+    n_all = sum_over_ranks(pg, local, float(full.size))
+    kern = max_over_ranks(pg, local, sum(kern_ms) / len(kern_ms))
+    tot = max_over_ranks(pg, local, sum(tot_ms) / len(tot_ms))
+    sims_s = n_all / (kern / 1e3)
+    # plain per-simulation path on a stride sample of the same sweep (rank 0)
+    plain = {}
+    if rank == 0:
+        sample = sweep_descs(G, seeds, cs_values, stride=997)
+        best = None
+        for slots in (6, 64, 256):
+            with make_batch() as b:
+                b.add_sims_array(sample, max_rule_bits=2)
+                dev_s = b.run_plain(slots)
+                r = b.results_array()
+            v = sample.size / dev_s
+            plain[f"slots{slots}_sims_per_s"] = v
+            best = v if best is None else max(best, v)
+        plain["best_sims_per_s"] = best
+        plain["sample"] = f"{sample.size} simulations (every 997th of the sweep)"
+    line = {
+        "metric": "search sims/s", "value": sims_s, "unit": "sims/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": kern, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "u4 (packed nibble states, bit-sliced integer logic)",
+        "data": "synthetic: reference cell hash, 30% fill of a centred 16^3 box, seeds 0..31",
+        "config": {"workload": f"49^3 FE sweep: 171 x 171 rules (<= 2 bits) x C in {{2,3,4,5}} x 32 seeds, "
+                               f"{T} ticks with early stop", "simulations": int(n_all),
+                   "parallelism": f"shards x{world}" if world > 1 else "single GPU",
+                   "l2": "grids resident in shared memory; initial grids read once per simulation"},
+        "cell_updates_per_s": ticks * G ** 3 * world / (kern / 1e3),
+        "categories": {"viable": int(cats[0]), "possible": int(cats[1]), "unviable": int(cats[2])},
+        "plain_path": plain,
+        "batched_over_plain": (sims_s / plain["best_sims_per_s"]) if plain else None,
+        "e2e": {"value": n_all / (tot / 1e3), "unit": "sims/s", "h2d_bytes_per_step": int(full.size * 16),
+                "d2h_bytes_per_step": int(full.size * cb.SIM_RESULT_DTYPE.itemsize)},
+        "gpu_launches": 4 * args.steps,
+    }
+    ctx.close()
+    return line
+
+
 def reference_arm(args, world, rank, local, pg):
     """The oracle port of the reference's CPU-free arithmetic on the host cores (no CPU stepping
     exists in the reference; its GPU path needs Vulkan, which this box does not have)."""
@@ -333,7 +446,10 @@ def main():
             print(json.dumps(line), flush=True)
         return
     world, rank, local, pg = dist_setup(args)
-    line = large_workload(args, world, rank, local, pg)
+    if args.workload == "sweep49":
+        line = sweep_workload(args, world, rank, local, pg)
+    else:
+        line = large_workload(args, world, rank, local, pg)
     if rank == 0 and line is not None:
         print(json.dumps(line), flush=True)
     if pg:

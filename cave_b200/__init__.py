@@ -123,6 +123,16 @@ def bitmask_to_rule_string(mask: int) -> str:
     return buf.value.decode()
 
 
+SIM_DESC_DTYPE = np.dtype([("birth", "<u8"), ("survival", "<u8"), ("shape", "<u8"), ("init", "<u4"),
+                           ("maxTicks", "<u4"), ("validTable", "<u4"), ("tag", "<u4")])
+SIM_RESULT_DTYPE = np.dtype([("info", "<u4", (6,)), ("category", "<u4"), ("tag", "<u4"), ("population", "<u4"),
+                             ("activeTicks", "<u4"), ("totalChanged", "<u8"), ("bbox_min", "<u4", (3,)),
+                             ("bbox_max", "<u4", (3,)), ("birth", "<u8"), ("survival", "<u8"), ("shape", "<u8"),
+                             ("error", "<u4"), ("pad", "<u4")])
+assert SIM_DESC_DTYPE.itemsize == ctypes.sizeof(SimDesc)
+assert SIM_RESULT_DTYPE.itemsize == ctypes.sizeof(SimResult)
+
+
 class Timing(ctypes.Structure):
     _fields_ = [("ticks", u32), ("launches", u32), ("tick_ms", ctypes.c_float), ("convert_ms", ctypes.c_float),
                 ("total_ms", ctypes.c_float)]
@@ -385,6 +395,19 @@ class Batch:
     def add_sims(self, descs, max_rule_bits=0):
         arr = (SimDesc * len(descs))(*descs)
         self.ctx.check(lib().cave_batch_add_sims(self.h, arr, len(descs), max_rule_bits), "cave_batch_add_sims")
+
+    def add_sims_array(self, arr: np.ndarray, max_rule_bits=0):
+        """Simulations from a numpy array of dtype SIM_DESC_DTYPE (same layout as cave_sim_desc)."""
+        assert arr.dtype == SIM_DESC_DTYPE and arr.flags["C_CONTIGUOUS"]
+        self.ctx.check(lib().cave_batch_add_sims(self.h, arr.ctypes.data_as(P(SimDesc)), arr.size, max_rule_bits),
+                       "cave_batch_add_sims")
+
+    def results_array(self) -> np.ndarray:
+        """All results as a numpy array of dtype SIM_RESULT_DTYPE."""
+        n = lib().cave_batch_size(self.h)
+        out = np.zeros(max(n, 1), dtype=SIM_RESULT_DTYPE)
+        self.ctx.check(lib().cave_batch_results(self.h, out.ctypes.data_as(P(SimResult)), n), "cave_batch_results")
+        return out[:n]
 
     def launch(self):
         self.ctx.check(lib().cave_batch_launch(self.h), "cave_batch_launch")

@@ -97,6 +97,8 @@ struct cave_batch {
     uint32_t* d_queues = nullptr;
     std::vector<cave_sim_params> translated;
     cudaEvent_t done = nullptr;
+    cudaEvent_t ev[4] = {};  // start of uploads, first kernel, after the last kernel, after read-back
+    uint32_t n_launches = 0;
     bool launched = false;
     uint64_t launched_n = 0;
     bool plain = false;                      // results came from cave_batch_run_plain
@@ -142,6 +144,12 @@ cave_status cave_batch_create(cave_ctx* ctx, cave_batch** out) {
         delete b;
         return CAVE_ERR_CUDA;
     }
+    for (auto& ev : b->ev) {
+        if (cudaEventCreate(&ev) != cudaSuccess) {
+            cave_batch_destroy(b);
+            return CAVE_ERR_CUDA;
+        }
+    }
     *out = b;
     return CAVE_OK;
 }
@@ -153,6 +161,8 @@ void cave_batch_destroy(cave_batch* b) {
     free_launch(b);
     cudaFree(b->pool);
     cudaEventDestroy(b->done);
+    for (auto& ev : b->ev)
+        if (ev) cudaEventDestroy(ev);
     delete b;
 }
 
@@ -285,6 +295,7 @@ cave_status cave_batch_launch(cave_batch* b) {
     }
     free_launch(b);
     cudaError_t e = cudaSuccess;
+    cudaEventRecord(b->ev[0], ctx->stream);
     if (n) {
         e = cudaMalloc(&b->d_rules, sizeof(DeviceRule) * std::max<size_t>(rules.size(), 1));
         if (e == cudaSuccess) e = cudaMalloc(&b->d_sims, sizeof(ResSim) * n);
@@ -298,6 +309,8 @@ cave_status cave_batch_launch(cave_batch* b) {
         if (e == cudaSuccess) e = cudaMemsetAsync(b->d_queues, 0, sizeof(uint32_t) * launches.size(), ctx->stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(b->d_results, 0, sizeof(cave_sim_result) * n, ctx->stream);
     }
+    if (e == cudaSuccess) e = cudaEventRecord(b->ev[1], ctx->stream);
+    b->n_launches = (uint32_t)launches.size();
     for (size_t li = 0; li < launches.size() && e == cudaSuccess; li++) {
         const Launch& L = launches[li];
         const size_t smem = resident_smem_bytes(L.P.X, L.P.Y, L.P.Z, L.P.nseg);
@@ -308,6 +321,7 @@ cave_status cave_batch_launch(cave_batch* b) {
         e = launch_resident((int)L.nb, (int)L.nt, L.P, b->d_sims + L.first, b->d_rules, b->pool, b->d_results,
                             b->d_queues + li, ctas, L.threads, ctx->stream);
     }
+    if (e == cudaSuccess) e = cudaEventRecord(b->ev[2], ctx->stream);
     if (e == cudaSuccess) e = cudaEventRecord(b->done, ctx->stream);
     if (e != cudaSuccess) return check_cuda(ctx, e, "cave_batch_launch");
     b->launched = true;
@@ -330,8 +344,17 @@ cave_status cave_batch_results(cave_batch* b, cave_sim_result* out, uint64_t n) 
     if (b->plain) {
         std::memcpy(out, b->host_results.data(), sizeof(cave_sim_result) * n);
     } else {
-        CAVE_CUDA(ctx, cudaEventSynchronize(b->done));
-        if (n) CAVE_CUDA(ctx, cudaMemcpy(out, b->d_results, sizeof(cave_sim_result) * n, cudaMemcpyDeviceToHost));
+        if (n)
+            CAVE_CUDA(ctx, cudaMemcpyAsync(out, b->d_results, sizeof(cave_sim_result) * n, cudaMemcpyDeviceToHost,
+                                           ctx->stream));
+        CAVE_CUDA(ctx, cudaEventRecord(b->ev[3], ctx->stream));
+        CAVE_CUDA(ctx, cudaEventSynchronize(b->ev[3]));
+        // device timing of the launch: kernels only, and uploads + kernels + read-back
+        cave_timing t{};
+        t.launches = b->n_launches;
+        cudaEventElapsedTime(&t.tick_ms, b->ev[1], b->ev[2]);
+        cudaEventElapsedTime(&t.total_ms, b->ev[0], b->ev[3]);
+        ctx->last_timing = t;
     }
     bool err = false;
     for (uint64_t i = 0; i < n; i++) {
