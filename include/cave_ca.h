@@ -104,7 +104,9 @@ const char* cave_last_error(const cave_ctx* ctx);
 /* Blocks until all work queued on the context's stream is done. */
 cave_status cave_ctx_synchronize(cave_ctx* ctx);
 
-/* Device-side timing of the last cave_step / cave_run call, measured with CUDA events on
+/* Device-side timing of the last cave_step / cave_run / cave_run_host call, or of the last
+ * batch whose results were read (tick_ms = its kernels, total_ms = uploads, kernels and
+ * read-back), measured with CUDA events on
  * the context's stream (replaces the reference's timestamp queries, queryManager.h:13-97).
  * Recorded only while enabled (off by default; it adds one event pair per phase). */
 typedef struct {
@@ -154,7 +156,8 @@ cave_status cave_step(cave_grid* g, const cave_sim_params* params, const uint64_
 /* ---- streaming path: many ticks in the library's bit-plane layout -------------------- */
 /* Same results as cave_step for the same inputs (every cell, every statistic), computed by
  * the z-slab streaming kernel: the grid is converted to a bit-plane layout once, stepped
- * nticks times (one launch per tick, captured in a CUDA graph) and converted back. The
+ * nticks times (one launch per tick, each allowed to start its prologue while the previous
+ * tick drains: programmatic dependent launch) and converted back. The
  * GridInfo of the manager shader (searchManager.slang:98-139) for those ticks is returned in
  * *info (may be NULL) with maxTicks as MAX_NUMBER_OF_TICKS_TO_SURVIVE; the run does not stop
  * on status > 0 (raw stepping). */
