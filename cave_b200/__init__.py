@@ -157,6 +157,8 @@ _SIGS = {
     "cave_ctx_last_timing": (i32, [ctypes.c_void_p, P(Timing)]),
     "cave_run_host": (i32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, u64, P(SimParams), P(u64), u32, u32,
                             u32, u32, P(TickStats), P(GridInfo)]),
+    "cave_run_noalloc": (i32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, u32, u32, u32, P(SimParams),
+                               P(u64), u32, u32, u32, u32, ctypes.c_void_p, P(GridInfo)]),
     "cave_grid_create": (i32, [ctypes.c_void_p, u32, u32, u32, P(ctypes.c_void_p)]),
     "cave_grid_destroy": (None, [ctypes.c_void_p]),
     "cave_grid_words": (u64, [u32, u32, u32]),
@@ -334,6 +336,23 @@ class Grid:
                                            nticks, nticks if max_ticks is None else max_ticks, pt,
                                            ctypes.byref(info)), "cave_run_host")
         return ([pt[i] for i in range(nticks)] if stats else None), info
+
+
+NOALLOC_SCRATCH_BYTES = 32 << 20
+
+
+def run_noalloc(ctx: Context, in_ptr, out_ptr, X, Y, Z, params: SimParams, nticks, max_ticks=None, valid=None,
+                max_rule_bits=0, per_tick_ptr=None) -> GridInfo:
+    """cave_run_noalloc: the streaming run on caller-owned device buffers (device addresses as
+    ints; per_tick_ptr: device array of nticks TickStats, or None). Allocates no device memory;
+    its scratch is one static array of NOALLOC_SCRATCH_BYTES per GPU. Returns the GridInfo."""
+    v = None if valid is None else np.ascontiguousarray(valid, dtype=np.uint64)
+    info = GridInfo()
+    ctx.check(lib().cave_run_noalloc(ctx.h, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr), X, Y, Z,
+                                     ctypes.byref(params), _u64p(v), 0 if v is None else v.size, max_rule_bits,
+                                     nticks, nticks if max_ticks is None else max_ticks,
+                                     ctypes.c_void_p(per_tick_ptr or 0), ctypes.byref(info)), "cave_run_noalloc")
+    return info
 
 
 def search_run(ctx: Context, config: SearchConfig, plain=False, sim_limit=0) -> SearchSummary:

@@ -174,6 +174,30 @@ cave_status cave_run_host(cave_grid* g, const uint32_t* in_words, uint32_t* out_
                           uint32_t maxRuleBits, uint32_t nticks, uint32_t maxTicks, cave_tick_stats* per_tick,
                           cave_grid_info* info);
 
+/* cave_run without any device allocation. No counterpart in the reference (its buffers are
+ * always created per slot, searchSystem.cpp:126-394); it exists for callers that must not
+ * allocate device memory while they run -- a serving loop whose HBM is held by another
+ * allocator, where cudaMalloc can fail, or that cannot take cudaFree's device-wide
+ * synchronisation between requests.
+ * d_in / d_out: caller-owned DEVICE buffers of cave_grid_words(X, Y, Z) words in the nibble
+ * layout (4-byte aligned; d_in == d_out is allowed). d_per_tick: caller-owned device array of
+ * nticks entries, or NULL. *info (host, may be NULL) receives the GridInfo as in cave_run.
+ * Cells, statistics and GridInfo equal cave_run's for the same inputs. Blocking.
+ * Scratch: one static device array of CAVE_NOALLOC_SCRATCH_BYTES per GPU, part of the
+ * library's device image (held by every GPU that loads the library until exit). A grid needs
+ * 32 bytes per 32 x-cells (rounded up) per row and plane plus a few KB; larger grids are
+ * rejected with CAVE_ERR_INVALID_ARG (256^3 and 320^3 fit). The first call on a device looks
+ * the array up (cudaGetSymbolAddress with that device current); make that first call before
+ * any stream capture. Every call on a device shares the array: calls that overlap on the GPU
+ * (two contexts, or two host threads, on one device) race and must be serialised by the
+ * caller. The simulation record in the array is rewritten by each call. Not timed by
+ * cave_ctx_set_timing. */
+#define CAVE_NOALLOC_SCRATCH_BYTES (32u << 20)
+cave_status cave_run_noalloc(cave_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t X, uint32_t Y,
+                             uint32_t Z, const cave_sim_params* params, const uint64_t* validBitmasks,
+                             uint32_t nValid, uint32_t maxRuleBits, uint32_t nticks, uint32_t maxTicks,
+                             cave_tick_stats* d_per_tick, cave_grid_info* info);
+
 /* ---- batched path: many small simulations ------------------------------------------ */
 /* One simulation of a batch: a rule run from an initial grid until the search manager
  * reports status > 0 (early death, or maxTicks reached), exactly the per-rule lifecycle of a
