@@ -25,6 +25,8 @@ import sys
 import tempfile
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -34,6 +36,8 @@ WORKLOADS = {
     "large256": (256, 1000),
     "large1024": (1024, 200),
     "sweep49": (49, 20),
+    "uneven2048": (0, 0),
+    "serve": (0, 0),
 }
 
 
@@ -47,6 +51,10 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ticks", type=int, default=0, help="override the workload's tick count (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--rate", type=float, default=200.0, help="serve: mean request arrivals per second")
+    ap.add_argument("--requests", type=int, default=64, help="serve: requests in the timed window")
+    ap.add_argument("--sims", type=int, default=2048, help="uneven2048: simulations in the batch")
+    ap.add_argument("--no-autotune", action="store_true")
     return ap.parse_args()
 
 
@@ -197,14 +205,12 @@ def large_workload(args, world, rank, local, pg):
     import torch
 
     import cave_b200 as cb
-    import oracle as O
 
     G, T = WORKLOADS[args.workload]
     T = args.ticks or T
     cells_per_step = G ** 3 * T
-    thr = O.threshold_from_float(0.40)
-    params_np = O.make_params(15, 0x7, 0x10, 0x18)
-    params = cb.SimParams(*[int(v) for v in params_np])
+    thr = cb.threshold_from_fill(0.40)
+    params = cb.make_params(15, 0x7, 0x10, 0x18)
     ctx = cb.Context(local)
     ctx.set_timing(True)
     g = cb.Grid(ctx, G, G, G)
@@ -285,6 +291,8 @@ def large_workload(args, world, rank, local, pg):
         "clocks": clocks,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        params_np = np.array([params.birthAndMaxCellStateRules, params.survivalAndNeighborhoodRules, 0],
+                             dtype=np.uint64)
         line["cpu_baseline"] = cpu_baseline_large(G, init_host, params_np)
     g.close()
     ctx.close()
@@ -324,11 +332,10 @@ def sweep_workload(args, world, rank, local, pg):
     import numpy as np
 
     import cave_b200 as cb
-    import oracle as O
 
     G, T = WORKLOADS["sweep49"]
     seeds, cs_values = 32, (2, 3, 4, 5)
-    thr = O.threshold_from_float(0.30)
+    thr = cb.threshold_from_fill(0.30)
     ctx = cb.Context(local)
     ctx.set_timing(True)
     vb = cb.valid_bitmasks(18, 2)
@@ -403,6 +410,227 @@ def sweep_workload(args, world, rank, local, pg):
     return line
 
 
+
+# ----------------------------------------------------------------------------- config 4 / 5 inputs
+NB_COUNT = {0x1: 6, 0x3: 18, 0x7: 26}
+
+
+def _rule_bits(g, n):
+    """1..4 distinct neighbour counts among 1..n as a reference rule mask (bit c-1 = count c)."""
+    k = int(g.integers(1, 5))
+    return sum(1 << int(c) for c in g.choice(n, size=k, replace=False))
+
+
+def uneven_sims(n, seed=20261203):
+    """The uneven-size batch: per simulation, in this draw order, edge from {33,49,65,97,129,193},
+    neighbourhood from {F, FE, Moore}, C from 2..16 (maxCellState C-1), survival and birth sets
+    of 1-4 counts, ticks from 10..500 and fill from [0.20, 0.50); spawn = the whole grid, seed =
+    the simulation index. numpy Generator over MT19937(seed)."""
+    g = np.random.Generator(np.random.MT19937(seed))
+    edges, flags = (33, 49, 65, 97, 129, 193), (0x1, 0x3, 0x7)
+    out = []
+    for i in range(n):
+        e = edges[int(g.integers(6))]
+        fl = flags[int(g.integers(3))]
+        C = int(g.integers(2, 17))
+        S = _rule_bits(g, NB_COUNT[fl])
+        B = _rule_bits(g, NB_COUNT[fl])
+        T = int(g.integers(10, 501))
+        p = float(g.uniform(0.20, 0.50))
+        out.append(dict(edge=e, flags=fl, maxcs=C - 1, birth=B, survival=S, ticks=T, fill=p, seed=i))
+    return out
+
+
+def uneven_workload(args, world, rank, local, pg):
+    import cave_b200 as cb
+
+    sims = uneven_sims(args.sims)
+    mine = sims[rank::world]
+    ctx = cb.Context(local)
+    ctx.set_timing(True)
+
+    def make_batch(subset, autotune):
+        b = cb.Batch(ctx)
+        b.set_options(autotune=autotune)
+        descs = []
+        for j, s in enumerate(subset):
+            ix = b.add_init_seeded(s["edge"], s["edge"], s["edge"], (s["edge"],) * 3, cb.threshold_from_fill(s["fill"]),
+                                   s["seed"], s["maxcs"])
+            descs.append(cb.SimDesc(cb.make_params(s["maxcs"], s["flags"], s["birth"], s["survival"]), ix, s["ticks"], 0,
+                                    j))
+        b.add_sims(descs)
+        return b
+
+    autotune = not args.no_autotune
+    tune_ms = 0.0
+    t0 = time.perf_counter()
+    for _ in range(args.warmup):
+        with make_batch(mine, autotune) as b:
+            b.launch()
+            b.results_array()
+            plan = b.plan()
+    tune_wall = time.perf_counter() - t0
+    barrier(pg, local)
+    kern_ms, tot_ms, wall = [], [], []
+    updates = 0
+    for _ in range(args.steps):
+        with make_batch(mine, autotune) as b:
+            w0 = time.perf_counter()
+            b.launch()
+            res = b.results_array()
+            wall.append(time.perf_counter() - w0)
+            t = ctx.last_timing()
+            kern_ms.append(t.tick_ms)
+            tot_ms.append(t.total_ms)
+            plan = b.plan()
+        vol = np.array([s["edge"] ** 3 for s in mine], dtype=np.int64)
+        updates = int((res["info"][:, 2].astype(np.int64) * vol).sum())
+        assert int(res["error"].max(initial=0)) == 0
+    barrier(pg, local)
+    kern = max_over_ranks(pg, local, sum(kern_ms) / len(kern_ms))
+    tot = max_over_ranks(pg, local, sum(tot_ms) / len(tot_ms))
+    n_all = sum_over_ranks(pg, local, float(len(mine)))
+    upd_all = sum_over_ranks(pg, local, float(updates))
+    # the plain per-simulation path (one launch per slot per tick, a host fence per tick) and
+    # the batched path on the same sample (every 64th simulation)
+    plain = {}
+    if rank == 0:
+        sample = sims[::64]
+        vol_s = np.array([s["edge"] ** 3 for s in sample], dtype=np.int64)
+        with make_batch(sample, autotune) as b:
+            dev_s = b.run_plain(len(sample))
+            r = b.results_array()
+        upd_s = int((r["info"][:, 2].astype(np.int64) * vol_s).sum())
+        with make_batch(sample, autotune) as b:
+            b.launch()
+            rb = b.results_array()
+            tb = ctx.last_timing().tick_ms / 1e3
+        assert np.array_equal(rb["info"], r["info"]), "plain and batched paths disagree"
+        plain = {"sample": f"{len(sample)} simulations (every 64th)", "plain_sims_per_s": len(sample) / dev_s,
+                 "plain_cell_updates_per_s": upd_s / dev_s, "batched_sims_per_s_same_sample": len(sample) / tb,
+                 "batched_cell_updates_per_s_same_sample": upd_s / tb, "batched_over_plain_same_sample": dev_s / tb}
+    line = {
+        "metric": "search sims/s", "value": n_all / (kern / 1e3), "unit": "sims/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": kern, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "u4 (packed nibble states, bit-sliced integer logic)",
+        "data": "synthetic: reference cell hash, 20-50% fill of the whole grid, seeds 0..2047",
+        "config": {"workload": f"uneven batch: {len(sims)} simulations, edges {{33,49,65,97,129,193}}, F/FE/Moore, "
+                               f"C 2..16, 1-4 counts per set, 10-500 ticks with early stop",
+                   "simulations": int(n_all), "autotune": autotune,
+                   "parallelism": f"shards x{world}" if world > 1 else "single GPU",
+                   "l2": "grids up to 65^3 resident in shared memory; larger grids in HBM (two copies each)"},
+        "cell_updates_per_s": upd_all / (kern / 1e3),
+        "plan": plan,
+        "autotune_and_warmup_wall_s": tune_wall,
+        "plain_path": plain,
+        "e2e": {"value": n_all / (tot / 1e3), "unit": "sims/s", "h2d_bytes_per_step": int(len(mine) * 40),
+                "d2h_bytes_per_step": int(len(mine) * cb.SIM_RESULT_DTYPE.itemsize)},
+        "host_wall_s_per_step": sum(wall) / len(wall),
+    }
+    ctx.close()
+    return line
+
+
+def serve_requests(n, rate, seed=20261204):
+    """Request stream: Poisson arrivals (mean `rate`/s); each request 1-256 simulations with
+    edge 32..256, ticks 10..500 and rules / fills as the uneven batch; spawn = whole grid."""
+    import cave_b200 as cb
+
+    g = np.random.Generator(np.random.MT19937(seed))
+    t, out = 0.0, []
+    flags = (0x1, 0x3, 0x7)
+    sid = 0
+    for _ in range(n):
+        t += float(g.exponential(1.0 / rate))
+        k = int(g.integers(1, 257))
+        r = cb.request_sims(k)
+        for i in range(k):
+            e = int(g.integers(32, 257))
+            fl = flags[int(g.integers(3))]
+            C = int(g.integers(2, 17))
+            S = _rule_bits(g, NB_COUNT[fl])
+            B = _rule_bits(g, NB_COUNT[fl])
+            p = cb.make_params(C - 1, fl, B, S)
+            r[i]["X"] = r[i]["Y"] = r[i]["Z"] = e
+            r[i]["maxTicks"] = int(g.integers(10, 501))
+            r[i]["birth"], r[i]["survival"] = p.birthAndMaxCellStateRules, p.survivalAndNeighborhoodRules
+            r[i]["spawnX"] = r[i]["spawnY"] = r[i]["spawnZ"] = e
+            r[i]["runSeedIndex"] = sid
+            r[i]["threshold"] = cb.threshold_from_fill(float(g.uniform(0.20, 0.50)))
+            r[i]["tag"] = i
+            sid += 1
+        out.append((t, r))
+    return out
+
+
+def serve_workload(args, world, rank, local, pg):
+    import cave_b200 as cb
+
+    reqs = serve_requests(args.requests, args.rate)[rank::world]
+    ctx = cb.Context(local)
+    budget = 120 * 10 ** 9
+    total_sims = sum(r.size for _, r in reqs)
+
+    def run(srv, timed_arrivals):
+        ids, lat = {}, []
+        t0 = time.perf_counter()
+        for t_arr, r in reqs:
+            if timed_arrivals:
+                d = t_arr - (time.perf_counter() - t0)
+                if d > 0:
+                    time.sleep(d)
+            ids[srv.submit(r)] = r.size
+        done = 0
+        upd = 0
+        while done < len(ids):
+            for rid in srv.poll():
+                res, l = srv.fetch(rid)
+                assert int(res["error"].max(initial=0)) == 0
+                lat.append(l)
+                done += 1
+            time.sleep(0.0005)
+        span = time.perf_counter() - t0
+        st = srv.stats()
+        return span, sorted(lat), st
+
+    with cb.Server(ctx, hbm_budget=budget, autotune=False) as srv:
+        warm = serve_requests(2, args.rate, seed=7)
+        for _, r in warm:
+            srv.wait(srv.submit(r), 600.0)
+        for rid in srv.poll():
+            pass
+    with cb.Server(ctx, hbm_budget=budget) as srv:
+        span_served, lat, st_served = run(srv, True)
+    with cb.Server(ctx, hbm_budget=budget) as srv:
+        span_off, _, st_off = run(srv, False)
+
+    def pct(p):
+        return lat[min(len(lat) - 1, int(p * (len(lat) - 1) + 0.5))] if lat else None
+
+    served_ups = st_served.cellUpdates / span_served
+    off_ups = st_off.cellUpdates / span_off
+    arrival_span = reqs[-1][0] if reqs else 0.0
+    line = {
+        "metric": "served cell-updates/s", "value": served_ups, "unit": "cell-updates/s", "n_gpus": world,
+        "steps": 1, "warmup": 1, "ms_per_step": span_served * 1e3, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "u4 (packed nibble states, bit-sliced integer logic)",
+        "data": "synthetic: Poisson request stream, reference cell hash seeding",
+        "config": {"workload": f"served: {len(reqs)} requests, Poisson {args.rate}/s, 1-256 sims each, edge 32..256, "
+                               f"ticks 10..500, F/FE/Moore, C 2..16", "requests": len(reqs), "simulations": total_sims,
+                   "hbm_budget_bytes": budget, "arrival_window_s": arrival_span},
+        "latency_p50_s": pct(0.50), "latency_p99_s": pct(0.99),
+        "server_p50_s": st_served.p50LatencySeconds, "server_p99_s": st_served.p99LatencySeconds,
+        "offline_cell_updates_per_s": off_ups, "throughput_loss_vs_offline": 1.0 - served_ups / off_ups,
+        "served_span_s": span_served, "offline_span_s": span_off, "peak_hbm_bytes": st_served.peakBytes,
+        "tick_launches": st_served.tickLaunches, "resident_launches": st_served.residentLaunches,
+        "rounds": st_served.rounds,
+        "e2e": {"value": served_ups, "unit": "cell-updates/s", "h2d_bytes_per_step": int(total_sims * 72),
+                "d2h_bytes_per_step": int(total_sims * cb.SIM_RESULT_DTYPE.itemsize)},
+    }
+    ctx.close()
+    return line
+
+
 def reference_arm(args, world, rank, local, pg):
     """The oracle port of the reference's CPU-free arithmetic on the host cores (no CPU stepping
     exists in the reference; its GPU path needs Vulkan, which this box does not have)."""
@@ -448,6 +676,10 @@ def main():
     world, rank, local, pg = dist_setup(args)
     if args.workload == "sweep49":
         line = sweep_workload(args, world, rank, local, pg)
+    elif args.workload == "uneven2048":
+        line = uneven_workload(args, world, rank, local, pg)
+    elif args.workload == "serve":
+        line = serve_workload(args, world, rank, local, pg)
     else:
         line = large_workload(args, world, rank, local, pg)
     if rank == 0 and line is not None:

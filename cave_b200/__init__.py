@@ -133,6 +133,28 @@ assert SIM_DESC_DTYPE.itemsize == ctypes.sizeof(SimDesc)
 assert SIM_RESULT_DTYPE.itemsize == ctypes.sizeof(SimResult)
 
 
+class BatchOptions(ctypes.Structure):
+    _fields_ = [("autotune", u32), ("tiledOnly", u32), ("ticksPerRound", u32), ("pad", u32), ("memoryBudget", u64)]
+
+
+class ServerOptions(ctypes.Structure):
+    _fields_ = [("hbmBudget", u64), ("maxInFlight", u32), ("ticksPerRound", u32), ("autotune", u32),
+                ("tiledOnly", u32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", u64), ("completed", u64), ("simsCompleted", u64), ("cellUpdates", u64),
+                ("p50LatencySeconds", ctypes.c_double), ("p99LatencySeconds", ctypes.c_double),
+                ("busySeconds", ctypes.c_double), ("peakBytes", u64), ("rounds", u64), ("tickLaunches", u64),
+                ("residentLaunches", u64), ("tuneMs", ctypes.c_double)]
+
+
+REQUEST_SIM_DTYPE = np.dtype([("X", "<u4"), ("Y", "<u4"), ("Z", "<u4"), ("maxTicks", "<u4"), ("birth", "<u8"),
+                              ("survival", "<u8"), ("shape", "<u8"), ("spawnX", "<u4"), ("spawnY", "<u4"),
+                              ("spawnZ", "<u4"), ("runSeedIndex", "<u4"), ("threshold", "<u8"), ("tag", "<u4"),
+                              ("pad", "<u4")])
+
+
 class Timing(ctypes.Structure):
     _fields_ = [("ticks", u32), ("launches", u32), ("tick_ms", ctypes.c_float), ("convert_ms", ctypes.c_float),
                 ("total_ms", ctypes.c_float)]
@@ -182,6 +204,15 @@ _SIGS = {
     "cave_batch_results": (i32, [ctypes.c_void_p, P(SimResult), u64]),
     "cave_batch_size": (u64, [ctypes.c_void_p]),
     "cave_batch_run_plain": (i32, [ctypes.c_void_p, u32, P(ctypes.c_double)]),
+    "cave_batch_set_options": (i32, [ctypes.c_void_p, P(BatchOptions)]),
+    "cave_batch_plan": (u64, [ctypes.c_void_p, ctypes.c_char_p, u64]),
+    "cave_server_create": (i32, [ctypes.c_void_p, P(ServerOptions), P(ctypes.c_void_p)]),
+    "cave_server_destroy": (None, [ctypes.c_void_p]),
+    "cave_server_submit": (i32, [ctypes.c_void_p, ctypes.c_void_p, u64, P(u64)]),
+    "cave_server_poll": (i32, [ctypes.c_void_p, P(u64), u64, P(u64)]),
+    "cave_server_wait": (i32, [ctypes.c_void_p, u64, ctypes.c_double]),
+    "cave_server_fetch": (i32, [ctypes.c_void_p, u64, ctypes.c_void_p, u64, P(ctypes.c_double)]),
+    "cave_server_get_stats": (i32, [ctypes.c_void_p, P(ServerStats)]),
     "cave_search_run": (i32, [ctypes.c_void_p, P(SearchConfig), u32, u64, P(SearchSummary)]),
     "cave_rule_string_to_bitmask": (u64, [ctypes.c_char_p]),
     "cave_bitmask_to_rule_string": (u64, [u64, ctypes.c_char_p, u64]),
@@ -219,6 +250,14 @@ def make_params(max_cell_state, flags, birth, survival, shape_id=0) -> SimParams
     """SimulationParameters with the simulation.h:58 maxCellState encoding."""
     return SimParams((((max_cell_state - 1) & 0xF) << 60) | (birth & PERM_MASK),
                      ((flags & 0xF) << 60) | (survival & PERM_MASK), shape_id & 0x1F)
+
+
+def threshold_from_fill(p: float) -> int:
+    """Fill threshold of the reference's raw-density seeding (searchSystem.cpp:260-262):
+    (uint32)((double)(float)p * 2^32); 2^32 (every cell of the box) for p >= 1."""
+    if p >= 1.0:
+        return 1 << 32
+    return int(float(np.float32(p)) * 4294967296.0) & 0xFFFFFFFF
 
 
 def grid_words(X, Y, Z) -> int:
@@ -428,6 +467,19 @@ class Batch:
         self.ctx.check(lib().cave_batch_results(self.h, out.ctypes.data_as(P(SimResult)), n), "cave_batch_results")
         return out[:n]
 
+    def set_options(self, autotune=False, tiled_only=False, ticks_per_round=0, memory_budget=0):
+        o = BatchOptions(1 if autotune else 0, 1 if tiled_only else 0, ticks_per_round, 0, memory_budget)
+        self.ctx.check(lib().cave_batch_set_options(self.h, ctypes.byref(o)), "cave_batch_set_options")
+
+    def plan(self):
+        """How each grid class of the last launch ran (list of dicts)."""
+        import json
+
+        n = lib().cave_batch_plan(self.h, None, 0)
+        buf = ctypes.create_string_buffer(n + 1)
+        lib().cave_batch_plan(self.h, buf, n + 1)
+        return json.loads(buf.value.decode() or "[]")
+
     def launch(self):
         self.ctx.check(lib().cave_batch_launch(self.h), "cave_batch_launch")
 
@@ -449,3 +501,67 @@ class Batch:
         out = (SimResult * max(n, 1))()
         self.ctx.check(lib().cave_batch_results(self.h, out, n), "cave_batch_results")
         return [out[i] for i in range(n)]
+
+
+def request_sims(n) -> np.ndarray:
+    """An empty request (numpy array of cave_request_sim)."""
+    return np.zeros(n, dtype=REQUEST_SIM_DTYPE)
+
+
+class Server:
+    """Sweep requests served as they arrive (cave_server): continuous batching on one GPU."""
+
+    def __init__(self, ctx: Context, hbm_budget=0, max_in_flight=0, ticks_per_round=0, autotune=False,
+                 tiled_only=False):
+        self.ctx = ctx
+        o = ServerOptions(hbm_budget, max_in_flight, ticks_per_round, 1 if autotune else 0, 1 if tiled_only else 0)
+        h = ctypes.c_void_p()
+        ctx.check(lib().cave_server_create(ctx.h, ctypes.byref(o), ctypes.byref(h)), "cave_server_create")
+        self.h = h
+        self.sizes = {}
+
+    def close(self):
+        if self.h:
+            lib().cave_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def submit(self, sims: np.ndarray) -> int:
+        assert sims.dtype == REQUEST_SIM_DTYPE and sims.flags["C_CONTIGUOUS"]
+        rid = u64()
+        self.ctx.check(lib().cave_server_submit(self.h, sims.ctypes.data, sims.size, ctypes.byref(rid)),
+                       "cave_server_submit")
+        self.sizes[rid.value] = sims.size
+        return rid.value
+
+    def poll(self, cap=4096):
+        ids = (u64 * cap)()
+        n = u64()
+        self.ctx.check(lib().cave_server_poll(self.h, ids, cap, ctypes.byref(n)), "cave_server_poll")
+        return [ids[i] for i in range(n.value)]
+
+    def wait(self, rid, timeout=0.0):
+        rc = lib().cave_server_wait(self.h, rid, timeout)
+        if rc == ERR_TIMEOUT:
+            return False
+        self.ctx.check(rc, "cave_server_wait")
+        return True
+
+    def fetch(self, rid):
+        """(results as SIM_RESULT_DTYPE array, latency seconds) of a completed request."""
+        n = self.sizes.pop(rid)
+        out = np.zeros(n, dtype=SIM_RESULT_DTYPE)
+        lat = ctypes.c_double()
+        self.ctx.check(lib().cave_server_fetch(self.h, rid, out.ctypes.data, n, ctypes.byref(lat)),
+                       "cave_server_fetch")
+        return out, lat.value
+
+    def stats(self) -> ServerStats:
+        st = ServerStats()
+        self.ctx.check(lib().cave_server_get_stats(self.h, ctypes.byref(st)), "cave_server_get_stats")
+        return st

@@ -9,15 +9,19 @@
 #include <algorithm>
 #include <cstring>
 #include <map>
+#include <memory>
+#include <thread>
 #include <new>
 #include <string>
 #include <tuple>
+#include <atomic>
 #include <unordered_map>
 #include <vector>
 
 #include "../../include/cave_ca.h"
 #include "context.h"
 #include "kernels.h"
+#include "engine.h"
 #include "rules.h"
 
 namespace cave {
@@ -46,39 +50,6 @@ struct RuleKeyHash {
     }
 };
 
-// Largest resident grid: strips * 16 B plus the exchange buffers must fit in shared memory.
-constexpr size_t kMaxResidentSmem = 220 * 1024;
-
-bool resident_fits(uint32_t X, uint32_t Y, uint32_t Z) {
-    const uint32_t SX = (X + 31u) / 32u;
-    uint32_t SXp = 1;
-    while (SXp < SX) SXp <<= 1;
-    if (SX > 32 || (uint64_t)Y * SXp > 1024) return false;
-    return resident_smem_bytes(X, Y, Z, 1) <= kMaxResidentSmem;
-}
-
-// Launch geometry of one resident class: segments of ~8-12 planes, <= 1024 threads.
-ResLaunch resident_geometry(uint32_t X, uint32_t Y, uint32_t Z, uint32_t& threads) {
-    ResLaunch P{};
-    P.X = X;
-    P.Y = Y;
-    P.Z = Z;
-    P.SX = (X + 31u) / 32u;
-    uint32_t SXp = 1, lg = 0;
-    while (SXp < P.SX) {
-        SXp <<= 1;
-        lg++;
-    }
-    P.sxp_log2 = lg;
-    const uint32_t cols = Y * SXp;
-    uint32_t nseg = std::max(1u, std::min<uint32_t>(1024u / cols, (Z + 7u) / 8u));
-    while (nseg > 1 && resident_smem_bytes(X, Y, Z, nseg) > kMaxResidentSmem) nseg--;
-    P.nseg = nseg;
-    P.seg_len = (Z + nseg - 1) / nseg;
-    threads = (nseg * cols + 31u) / 32u * 32u;
-    return P;
-}
-
 }  // namespace cave
 
 using namespace cave;
@@ -103,6 +74,15 @@ struct cave_batch {
     uint64_t launched_n = 0;
     bool plain = false;                      // results came from cave_batch_run_plain
     std::vector<cave_sim_result> host_results;
+    cave_batch_options opt{};
+    // tiled simulations: the engine, driven by a worker thread until they have all finished
+    std::unique_ptr<Engine> engine;
+    std::thread worker;
+    std::atomic<bool> worker_done{true};
+    cave_status worker_rc = CAVE_OK;
+    std::vector<cudaStream_t> streams;       // resident launches of different classes overlap
+    std::string plan;
+    double tune_ms = 0;
 };
 
 static cave_status reserve_pool(cave_batch* b, uint64_t strips) {
@@ -157,6 +137,12 @@ cave_status cave_batch_create(cave_ctx* ctx, cave_batch** out) {
 void cave_batch_destroy(cave_batch* b) {
     if (!b) return;
     cudaSetDevice(b->ctx->device);
+    if (b->worker.joinable()) b->worker.join();
+    b->engine.reset();
+    for (cudaStream_t st : b->streams) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    }
     cudaStreamSynchronize(b->ctx->stream);
     free_launch(b);
     cudaFree(b->pool);
@@ -260,16 +246,71 @@ cave_status cave_batch_launch(cave_batch* b) {
         }
         sim_rule[i] = it->second;
     }
-    // classes: (grid shape, neighbourhood, term count)
-    using ClassKey = std::tuple<uint32_t, uint32_t, uint32_t, uint32_t, uint32_t>;
-    std::map<ClassKey, std::vector<uint32_t>> classes;
+    // execution choice per class (grid shape, neighbourhood): resident or tiled, tile shape
+    std::map<TuneKey, ExecChoice> choice;
+    std::vector<uint8_t> is_res(n, 0);
+    uint64_t tiled_bytes = 0, tiled_max = 0;
     for (uint64_t i = 0; i < n; i++) {
         const InitGrid& g = b->inits[b->sims[i].d.init];
-        if (!resident_fits(g.X, g.Y, g.Z))
-            return set_error(ctx, CAVE_ERR_INVALID_ARG,
-                             "batched simulation grid too large for shared memory (use cave_run per grid)");
         const DeviceRule& r = rules[sim_rule[i]];
-        classes[ClassKey{g.X, g.Y, g.Z, r.flags & 7u, r.nterms}].push_back((uint32_t)i);
+        const TuneKey key{g.X, g.Y, g.Z, r.flags & 7u};
+        auto it = choice.find(key);
+        if (it == choice.end()) {
+            EngineSim probe;
+            probe.rule = r;
+            probe.nb = r.flags & 7u;
+            probe.nt = r.nterms;
+            probe.X = g.X;
+            probe.Y = g.Y;
+            probe.Z = g.Z;
+            probe.init = b->pool + g.offset;
+            it = choice.emplace(key, choose_exec(ctx, ctx->stream, probe, b->opt.tiledOnly != 0, b->opt.autotune != 0,
+                                                 &b->tune_ms)).first;
+        }
+        is_res[i] = it->second.resident ? 1 : 0;
+        if (!is_res[i]) {
+            const uint64_t need = ((2 * (uint64_t)((g.X + 31) / 32) * g.Y * g.Z * 16) + 255) / 256 * 256;
+            tiled_bytes += need;
+            tiled_max = std::max(tiled_max, need);
+        }
+    }
+    {
+        b->plan = "[";
+        bool first = true;
+        for (const auto& [k, c] : choice) {
+            b->plan += std::string(first ? "" : ",") + "{\"grid\":[" + std::to_string(k.X) + "," + std::to_string(k.Y) + "," +
+                       std::to_string(k.Z) + "],\"nb\":" + std::to_string(k.nb) + ",\"path\":\"" +
+                       (c.resident ? "resident\",\"nseg\":" + std::to_string(c.nseg)
+                                   : "tiled\",\"rows\":" + std::to_string(c.rows) + ",\"log2_cells_per_cta\":" +
+                                         std::to_string(c.cells ? c.cells : 18)) +
+                       "}";
+            first = false;
+        }
+        b->plan += "]";
+    }
+    // resident classes: (grid shape, neighbourhood, term count, z-segments)
+    using ClassKey = std::tuple<uint32_t, uint32_t, uint32_t, uint32_t, uint32_t, uint32_t>;
+    std::map<ClassKey, std::vector<uint32_t>> classes;
+    std::vector<EngineSim> tiled;
+    for (uint64_t i = 0; i < n; i++) {
+        const InitGrid& g = b->inits[b->sims[i].d.init];
+        const DeviceRule& r = rules[sim_rule[i]];
+        if (is_res[i]) {
+            const ExecChoice& c = choice[TuneKey{g.X, g.Y, g.Z, r.flags & 7u}];
+            classes[ClassKey{g.X, g.Y, g.Z, r.flags & 7u, r.nterms, c.nseg}].push_back((uint32_t)i);
+        } else {
+            EngineSim es;
+            es.key = i;
+            es.rule = r;
+            es.nb = r.flags & 7u;
+            es.nt = r.nterms;
+            es.X = g.X;
+            es.Y = g.Y;
+            es.Z = g.Z;
+            es.max_ticks = b->sims[i].d.maxTicks;
+            es.init = b->pool + g.offset;
+            tiled.push_back(es);
+        }
     }
     std::vector<ResSim> rs;
     rs.reserve(n);
@@ -281,7 +322,7 @@ cave_status cave_batch_launch(cave_batch* b) {
     for (auto& [key, idx] : classes) {
         Launch L{};
         uint32_t threads = 0;
-        L.P = resident_geometry(std::get<0>(key), std::get<1>(key), std::get<2>(key), threads);
+        L.P = resident_geometry(std::get<0>(key), std::get<1>(key), std::get<2>(key), std::get<5>(key), threads);
         L.P.n_sims = (uint32_t)idx.size();
         L.nb = std::get<3>(key);
         L.nt = std::get<4>(key);
@@ -289,48 +330,128 @@ cave_status cave_batch_launch(cave_batch* b) {
         L.first = (uint32_t)rs.size();
         for (uint32_t i : idx) {
             const PendingSim& ps = b->sims[i];
-            rs.push_back(ResSim{sim_rule[i], (uint32_t)b->inits[ps.d.init].offset, ps.d.maxTicks, i});
+            rs.push_back(ResSim{b->pool + b->inits[ps.d.init].offset, sim_rule[i], ps.d.maxTicks, i, 0u});
         }
         launches.push_back(L);
+    }
+    // the tiled engine: a cell pool for the tiled simulations (all at once when the budget
+    // allows, else admitted in waves as earlier ones finish)
+    if (!tiled.empty()) {
+        uint64_t budget = b->opt.memoryBudget;
+        if (!budget) {
+            size_t fr = 0, tot = 0;
+            CAVE_CUDA(ctx, cudaMemGetInfo(&fr, &tot));
+            budget = fr / 2;
+        }
+        EngineConfig ec;
+        ec.pool_bytes = std::max(std::min(tiled_bytes, budget), tiled_max);
+        ec.max_slots = (uint32_t)std::min<uint64_t>(tiled.size(), 1u << 16);
+        ec.ticks_per_round = b->opt.ticksPerRound ? b->opt.ticksPerRound : 8u;
+        ec.tiled_only = 1;
+        ec.autotune = b->opt.autotune;
+        b->engine = std::make_unique<Engine>(ctx);
+        cave_status rc = b->engine->init(ec);
+        if (rc == CAVE_OK) rc = b->engine->submit(tiled);
+        if (rc) {
+            b->engine.reset();
+            return rc;
+        }
     }
     free_launch(b);
     cudaError_t e = cudaSuccess;
     cudaEventRecord(b->ev[0], ctx->stream);
     if (n) {
         e = cudaMalloc(&b->d_rules, sizeof(DeviceRule) * std::max<size_t>(rules.size(), 1));
-        if (e == cudaSuccess) e = cudaMalloc(&b->d_sims, sizeof(ResSim) * n);
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_sims, sizeof(ResSim) * std::max<size_t>(rs.size(), 1));
         if (e == cudaSuccess) e = cudaMalloc(&b->d_results, sizeof(cave_sim_result) * n);
-        if (e == cudaSuccess) e = cudaMalloc(&b->d_queues, sizeof(uint32_t) * launches.size());
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_queues, sizeof(uint32_t) * std::max<size_t>(launches.size(), 1));
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(b->d_rules, rules.data(), sizeof(DeviceRule) * rules.size(), cudaMemcpyHostToDevice,
                                 ctx->stream);
+        if (e == cudaSuccess && !rs.empty())
+            e = cudaMemcpyAsync(b->d_sims, rs.data(), sizeof(ResSim) * rs.size(), cudaMemcpyHostToDevice, ctx->stream);
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(b->d_sims, rs.data(), sizeof(ResSim) * n, cudaMemcpyHostToDevice, ctx->stream);
-        if (e == cudaSuccess) e = cudaMemsetAsync(b->d_queues, 0, sizeof(uint32_t) * launches.size(), ctx->stream);
+            e = cudaMemsetAsync(b->d_queues, 0, sizeof(uint32_t) * std::max<size_t>(launches.size(), 1), ctx->stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(b->d_results, 0, sizeof(cave_sim_result) * n, ctx->stream);
     }
     if (e == cudaSuccess) e = cudaEventRecord(b->ev[1], ctx->stream);
     b->n_launches = (uint32_t)launches.size();
+    // resident classes run on a few streams so that small classes share the GPU
+    if (launches.size() > 1 && b->streams.empty()) {
+        b->streams.resize(4);
+        for (auto& st : b->streams)
+            if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    }
     for (size_t li = 0; li < launches.size() && e == cudaSuccess; li++) {
         const Launch& L = launches[li];
-        const size_t smem = resident_smem_bytes(L.P.X, L.P.Y, L.P.Z, L.P.nseg);
-        // resident CTAs per SM: bounded by shared memory (228 KB per SM, 1 KB reserved per CTA)
-        const uint32_t per_sm = std::max<uint32_t>(1u, (uint32_t)((228u * 1024u) / (smem + 3 * 1024u)));
-        const uint32_t by_threads = std::max<uint32_t>(1u, 2048u / L.threads);
-        const uint32_t ctas = std::min<uint64_t>((uint64_t)ctx->sm_count * std::min(per_sm, by_threads), L.P.n_sims);
-        e = launch_resident((int)L.nb, (int)L.nt, L.P, b->d_sims + L.first, b->d_rules, b->pool, b->d_results,
-                            b->d_queues + li, ctas, L.threads, ctx->stream);
+        cudaStream_t st = launches.size() > 1 ? b->streams[li % b->streams.size()] : ctx->stream;
+        if (st != ctx->stream && li < b->streams.size()) e = cudaStreamWaitEvent(st, b->ev[1], 0);
+        const uint32_t ctas =
+            std::min<uint64_t>((uint64_t)ctx->sm_count * resident_ctas_per_sm(L.P, L.threads), L.P.n_sims);
+        if (e == cudaSuccess)
+            e = launch_resident((int)L.nb, (int)L.nt, L.P, b->d_sims + L.first, b->d_rules, b->d_results,
+                                b->d_queues + li, nullptr, ctas, L.threads, st);
     }
-    if (e == cudaSuccess) e = cudaEventRecord(b->ev[2], ctx->stream);
-    if (e == cudaSuccess) e = cudaEventRecord(b->done, ctx->stream);
+    if (launches.size() > 1)
+        for (size_t i = 0; i < b->streams.size() && i < launches.size() && e == cudaSuccess; i++) {
+            cudaEvent_t j;
+            e = cudaEventCreateWithFlags(&j, cudaEventDisableTiming);
+            if (e == cudaSuccess) e = cudaEventRecord(j, b->streams[i]);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, j, 0);
+            cudaEventDestroy(j);
+        }
     if (e != cudaSuccess) return check_cuda(ctx, e, "cave_batch_launch");
     b->launched = true;
     b->launched_n = n;
+    if (b->engine) {
+        // the worker runs the tiled rounds; when they are done it closes the timed region
+        e = cudaEventRecord(b->ev[3], ctx->stream);  // initial grids and uploads are in place
+        if (e == cudaSuccess && b->engine->after(b->ev[3]) != CAVE_OK) e = cudaErrorUnknown;
+        if (e != cudaSuccess) return check_cuda(ctx, e, "cave_batch_launch");
+        b->worker_done = false;
+        b->worker_rc = CAVE_OK;
+        b->worker = std::thread([b]() {
+            cudaSetDevice(b->ctx->device);
+            cave_status rc = b->engine->run_until_idle();
+            cudaEvent_t fin = nullptr;
+            if (rc == CAVE_OK && cudaEventCreateWithFlags(&fin, cudaEventDisableTiming) == cudaSuccess) {
+                b->engine->record_end(fin);
+                cudaStreamWaitEvent(b->ctx->stream, fin, 0);
+                cudaEventDestroy(fin);
+            }
+            cudaEventRecord(b->ev[2], b->ctx->stream);
+            cudaEventRecord(b->done, b->ctx->stream);
+            b->worker_rc = rc;
+            b->worker_done = true;
+        });
+    } else {
+        e = cudaEventRecord(b->ev[2], ctx->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(b->done, ctx->stream);
+        if (e != cudaSuccess) return check_cuda(ctx, e, "cave_batch_launch");
+    }
     return CAVE_OK;
+}
+
+cave_status cave_batch_set_options(cave_batch* b, const cave_batch_options* o) {
+    if (!b || !o) return CAVE_ERR_INVALID_ARG;
+    if (b->launched) return set_error(b->ctx, CAVE_ERR_INVALID_ARG, "batch already launched");
+    b->opt = *o;
+    return CAVE_OK;
+}
+
+uint64_t cave_batch_plan(const cave_batch* b, char* out, uint64_t cap) {
+    if (!b) return 0;
+    if (out && cap) {
+        const uint64_t n = std::min<uint64_t>(cap - 1, b->plan.size());
+        std::memcpy(out, b->plan.data(), n);
+        out[n] = 0;
+    }
+    return b->plan.size();
 }
 
 cave_status cave_batch_poll(cave_batch* b) {
     if (!b || !b->launched) return CAVE_ERR_INVALID_ARG;
+    if (!b->worker_done) return CAVE_ERR_NOT_READY;
     const cudaError_t e = cudaEventQuery(b->done);
     if (e == cudaErrorNotReady) return CAVE_ERR_NOT_READY;
     if (e != cudaSuccess) return check_cuda(b->ctx, e, "cave_batch_poll");
@@ -341,6 +462,8 @@ cave_status cave_batch_results(cave_batch* b, cave_sim_result* out, uint64_t n) 
     if (!b || !b->launched || (n && !out) || n > b->launched_n) return CAVE_ERR_INVALID_ARG;
     cave_ctx* ctx = b->ctx;
     CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (b->worker.joinable()) b->worker.join();
+    if (b->worker_rc) return b->worker_rc;
     if (b->plain) {
         std::memcpy(out, b->host_results.data(), sizeof(cave_sim_result) * n);
     } else {
@@ -355,6 +478,15 @@ cave_status cave_batch_results(cave_batch* b, cave_sim_result* out, uint64_t n) 
         cudaEventElapsedTime(&t.tick_ms, b->ev[1], b->ev[2]);
         cudaEventElapsedTime(&t.total_ms, b->ev[0], b->ev[3]);
         ctx->last_timing = t;
+        if (b->engine) {  // tiled simulations report through the engine (key = queue index)
+            std::vector<EngineResult> er;
+            b->engine->take_results(er);
+            for (const EngineResult& r : er)
+                if (r.key < n) out[r.key] = r.result;
+            const EngineStats es = b->engine->stats();
+            ctx->last_timing.launches += (uint32_t)std::min<uint64_t>(es.tick_launches + es.resident_launches + es.rounds,
+                                                                      0xFFFFFFFFu);
+        }
     }
     bool err = false;
     for (uint64_t i = 0; i < n; i++) {

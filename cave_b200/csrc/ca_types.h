@@ -37,6 +37,8 @@ struct DeviceRule {
     RuleTerm terms[kMaxTerms];
 };
 
+static_assert(sizeof(DeviceRule) % 16 == 0, "DeviceRule arrays keep 16-byte alignment (copied as uint4)");
+
 // Count planes needed per neighbourhood (max count: F 7, E 12, FE 19, C 8, FC 15, EC 20,
 // FEC 27, where the F-containing ones include the cell itself); nb = 0 counts nothing.
 CAVE_HD constexpr int count_bits(int nb) {

@@ -80,6 +80,25 @@ CAVE_HD inline void manager_update(const cave_grid_snapshot& snap, cave_grid_inf
     }
 }
 
+// ---- completion ring -------------------------------------------------------------------
+// Finished simulations of the engine (batched and served runs) are reported through a ring
+// whose entries live in host-mapped pinned memory: the device writes the result, fences at
+// system scope and then writes `seq`; the host reads entries in order, an entry being ready
+// once its seq equals its index + 1. Indices come from `count` (device memory). The engine
+// never has more simulations in flight than the ring has entries, so no entry is overwritten
+// before the host has read it.
+struct DoneEntry {
+    cave_sim_result result;
+    uint32_t slot;             // engine slot of the simulation
+    uint32_t seq;              // index + 1, written last
+};
+static_assert(sizeof(DoneEntry) == 112, "DoneEntry layout");
+struct DoneRing {
+    uint32_t count;            // next entry index (device memory, atomic)
+    uint32_t cap;
+    DoneEntry* entries;        // device alias of the host-mapped entry array
+};
+
 // ---- bit-plane (strip) path -----------------------------------------------------------
 // Per-simulation device record of the strip kernels.
 struct StripSim {
@@ -104,7 +123,9 @@ struct StripSim {
     uint64_t total_changed;
     cave_tick_stats last;
     cave_tick_stats* per_tick;  // optional, tick_limit entries
-    uint64_t pad;
+    DoneRing* ring;             // optional: the final result is pushed here when done
+    uint32_t slot;              // engine slot reported with the result
+    uint32_t pad;
 };
 
 }  // namespace cave

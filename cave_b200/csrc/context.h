@@ -3,12 +3,36 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
 
 #include "cave_internal.h"
 #include "kernels.h"
+
+namespace cave {
+// How one simulation class is executed (chosen by the autotuner or by defaults).
+struct ExecChoice {
+    uint32_t resident = 0;   // 1: resident kernel, 0: tiled
+    uint32_t nseg = 0;       // resident: z-segments per CTA (0 = default geometry)
+    uint32_t rows = 0;       // tiled: rows per CTA incl. the two halo rows (0 = default)
+    uint32_t cells = 0;      // tiled: log2 of the target cells per CTA (0 = default)
+    bool operator==(const ExecChoice& o) const {
+        return resident == o.resident && nseg == o.nseg && rows == o.rows && cells == o.cells;
+    }
+};
+// Tuning-cache key: grid shape and neighbourhood bits.
+struct TuneKey {
+    uint32_t X, Y, Z, nb;
+    bool operator<(const TuneKey& o) const {
+        if (X != o.X) return X < o.X;
+        if (Y != o.Y) return Y < o.Y;
+        if (Z != o.Z) return Z < o.Z;
+        return nb < o.nb;
+    }
+};
+}  // namespace cave
 
 struct cave_ctx {
     int device = 0;
@@ -19,6 +43,9 @@ struct cave_ctx {
     bool timing = false;
     cudaEvent_t ev[6] = {};  // created when timing is enabled
     cave_timing last_timing = {};
+    // autotuner results, shared by every batch and server of the context
+    std::mutex tune_mu;
+    std::map<cave::TuneKey, cave::ExecChoice> tune_cache;
 };
 
 struct cave_grid {

@@ -42,24 +42,43 @@ struct ResLaunch {           // geometry shared by every simulation of one launc
     uint32_t nseg, seg_len;  // z-segments per CTA and planes per segment
     uint32_t n_sims;
 };
-struct ResSim {              // one simulation of a resident launch
+struct ResSim {              // one simulation of a resident launch (24 bytes)
+    const uint4* init;       // initial grid (strip layout, device memory, 16-byte aligned)
     uint32_t rule;           // index into the DeviceRule table
-    uint32_t init;           // offset (in strips) of the initial grid in the initial-grid pool
     uint32_t max_ticks;
-    uint32_t result;         // index into the result array
+    uint32_t result;         // index into the result array, or the slot reported to the ring
+    uint32_t pad;
 };
 size_t resident_smem_bytes(uint32_t X, uint32_t Y, uint32_t Z, uint32_t nseg);
 // nt: sparse term count of every rule in the launch (0 = mux tree), nb: neighbourhood bits.
+// ring: when set, each finished simulation is pushed to it (slot = ResSim::result) instead of
+// being written to results.
 cudaError_t launch_resident(int nb, int nt, const ResLaunch& P, const ResSim* sims, const DeviceRule* rules,
-                            const uint4* inits, cave_sim_result* results, uint32_t* queue, uint32_t ctas,
+                            cave_sim_result* results, uint32_t* queue, DoneRing* ring, uint32_t ctas,
                             uint32_t threads, cudaStream_t st);
+
+// ---- engine set-up
+// One initial grid to place at byte offset `dst` of the engine's cell pool: a copy of `src`
+// (strip layout, n_strips strips) when src is set, else seeded by `seed`.
+struct EngineJob {
+    const uint4* src;
+    uint64_t dst;
+    uint64_t n_strips;
+    SeedSpec seed;
+};
+// Installs n_recs staged records at recs[rec_slots[i]] and runs every job, in one launch.
+cudaError_t launch_engine_setup(const EngineJob* jobs, uint32_t n_jobs, uint64_t max_strips, uint4* pool,
+                                const StripSim* recs_in, const uint32_t* rec_slots, uint32_t n_recs, StripSim* recs,
+                                cudaStream_t st);
 
 // threads = rows * SXp (rows includes the two halo rows), SXp = power of two >= SX, <= 32.
 // nt: sparse term count of the rule (0 = mux tree). param_rule: the rule of every item's
 // simulation when the launch holds one simulation only (passed as a kernel parameter), else null.
 // Launches use programmatic dependent launch, so consecutive ticks overlap set-up and drain.
+// pdl = false launches without the programmatic-dependent-launch attribute (the first tick
+// after a cross-stream event wait).
 cudaError_t launch_stream_tick(int nb, int nt, const DeviceRule* param_rule, const StreamItem* items,
                                uint32_t n_items, StripSim* sims, uint4* pool, uint32_t SX, uint32_t SXp,
-                               uint32_t threads, cudaStream_t st);
+                               uint32_t threads, cudaStream_t st, bool pdl = true);
 
 }  // namespace cave

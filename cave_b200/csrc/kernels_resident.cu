@@ -22,6 +22,7 @@
 #include "cave_internal.h"
 #include "kernels.h"
 #include "ptx.cuh"
+#include "ring.cuh"
 
 namespace cave {
 
@@ -36,10 +37,11 @@ __device__ __forceinline__ uint4 to_u4(const uint32_t* p) {
 
 template <int NB, int NT>
 __global__ void __launch_bounds__(1024) k_resident(ResLaunch P, const ResSim* __restrict__ sims,
-                                                   const DeviceRule* __restrict__ rules, const uint4* __restrict__ inits,
-                                                   cave_sim_result* __restrict__ results, uint32_t* queue) {
+                                                   const DeviceRule* __restrict__ rules,
+                                                   cave_sim_result* __restrict__ results, uint32_t* queue,
+                                                   DoneRing* ring) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ DeviceRule s_rule;
+    __shared__ __align__(16) DeviceRule s_rule;  // filled with 16-byte copies
     __shared__ uint32_t s_sim, s_stop;
     __shared__ uint32_t red[32][11];
     __shared__ __align__(8) uint64_t s_bar;
@@ -92,7 +94,7 @@ __global__ void __launch_bounds__(1024) k_resident(ResLaunch P, const ResSim* __
         if (tid == 0) {
             fence_proxy_async();
             mbar_expect_tx(&s_bar, grid_bytes);
-            bulk_g2s(grid, inits + (size_t)sd.init, grid_bytes, &s_bar);
+            bulk_g2s(grid, sd.init, grid_bytes, &s_bar);
         }
         uint32_t err = 0;
         if (!mbar_wait_bounded(&s_bar, bar_phase, kSpinLimit)) err = kErrWaitTimeout;
@@ -220,8 +222,7 @@ __global__ void __launch_bounds__(1024) k_resident(ResLaunch P, const ResSim* __
         if (tid == 0) {
             cave_sim_result r;
             r.info = info;
-            const uint32_t maxcs = s_rule.maxcs;
-            r.category = info.status == 2 ? 0u : ((uint64_t)info.numberOfSimulationTicksSurvived > (uint64_t)maxcs + 1 ? 1u : 2u);
+            r.category = result_category(info, s_rule.maxcs);
             r.tag = 0;
             r.population = last_pop;
             r.activeTicks = active_ticks;
@@ -233,7 +234,10 @@ __global__ void __launch_bounds__(1024) k_resident(ResLaunch P, const ResSim* __
             r.params = cave_sim_params{0, 0, 0};
             r.error = err;
             r.pad = 0;
-            results[sd.result] = r;
+            if (ring)
+                ring_push(ring, sd.result, r);
+            else
+                results[sd.result] = r;
         }
         __syncthreads();  // grid and rule buffers are reused by the next simulation
     }
@@ -247,43 +251,43 @@ size_t resident_smem_bytes(uint32_t X, uint32_t Y, uint32_t Z, uint32_t nseg) {
 }
 
 template <int NB, int NT>
-static cudaError_t launch_res_inst(const ResLaunch& P, const ResSim* sims, const DeviceRule* rules, const uint4* inits,
-                                   cave_sim_result* results, uint32_t* queue, uint32_t ctas, uint32_t threads,
-                                   size_t smem, cudaStream_t st) {
+static cudaError_t launch_res_inst(const ResLaunch& P, const ResSim* sims, const DeviceRule* rules,
+                                   cave_sim_result* results, uint32_t* queue, DoneRing* ring, uint32_t ctas,
+                                   uint32_t threads, size_t smem, cudaStream_t st) {
     auto k = k_resident<NB, NT>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k<<<ctas, threads, smem, st>>>(P, sims, rules, inits, results, queue);
+    k<<<ctas, threads, smem, st>>>(P, sims, rules, results, queue, ring);
     return cudaGetLastError();
 }
 
 template <int NB>
 static cudaError_t launch_res_nb(int nt, const ResLaunch& P, const ResSim* sims, const DeviceRule* rules,
-                                 const uint4* inits, cave_sim_result* results, uint32_t* queue, uint32_t ctas,
-                                 uint32_t threads, size_t smem, cudaStream_t st) {
+                                 cave_sim_result* results, uint32_t* queue, DoneRing* ring,
+                                 uint32_t ctas, uint32_t threads, size_t smem, cudaStream_t st) {
     switch (nt) {
-        case 0: return launch_res_inst<NB, 0>(P, sims, rules, inits, results, queue, ctas, threads, smem, st);
-        case 1: return launch_res_inst<NB, 1>(P, sims, rules, inits, results, queue, ctas, threads, smem, st);
-        case 2: return launch_res_inst<NB, 2>(P, sims, rules, inits, results, queue, ctas, threads, smem, st);
-        case 3: return launch_res_inst<NB, 3>(P, sims, rules, inits, results, queue, ctas, threads, smem, st);
-        case 4: return launch_res_inst<NB, 4>(P, sims, rules, inits, results, queue, ctas, threads, smem, st);
+        case 0: return launch_res_inst<NB, 0>(P, sims, rules, results, queue, ring, ctas, threads, smem, st);
+        case 1: return launch_res_inst<NB, 1>(P, sims, rules, results, queue, ring, ctas, threads, smem, st);
+        case 2: return launch_res_inst<NB, 2>(P, sims, rules, results, queue, ring, ctas, threads, smem, st);
+        case 3: return launch_res_inst<NB, 3>(P, sims, rules, results, queue, ring, ctas, threads, smem, st);
+        case 4: return launch_res_inst<NB, 4>(P, sims, rules, results, queue, ring, ctas, threads, smem, st);
         default: return cudaErrorInvalidValue;
     }
 }
 
 cudaError_t launch_resident(int nb, int nt, const ResLaunch& P, const ResSim* sims, const DeviceRule* rules,
-                            const uint4* inits, cave_sim_result* results, uint32_t* queue, uint32_t ctas,
+                            cave_sim_result* results, uint32_t* queue, DoneRing* ring, uint32_t ctas,
                             uint32_t threads, cudaStream_t st) {
     const size_t smem = resident_smem_bytes(P.X, P.Y, P.Z, P.nseg);
     switch (nb & 7) {
-        case 0: return launch_res_nb<0>(nt, P, sims, rules, inits, results, queue, ctas, threads, smem, st);
-        case 1: return launch_res_nb<1>(nt, P, sims, rules, inits, results, queue, ctas, threads, smem, st);
-        case 2: return launch_res_nb<2>(nt, P, sims, rules, inits, results, queue, ctas, threads, smem, st);
-        case 3: return launch_res_nb<3>(nt, P, sims, rules, inits, results, queue, ctas, threads, smem, st);
-        case 4: return launch_res_nb<4>(nt, P, sims, rules, inits, results, queue, ctas, threads, smem, st);
-        case 5: return launch_res_nb<5>(nt, P, sims, rules, inits, results, queue, ctas, threads, smem, st);
-        case 6: return launch_res_nb<6>(nt, P, sims, rules, inits, results, queue, ctas, threads, smem, st);
-        case 7: return launch_res_nb<7>(nt, P, sims, rules, inits, results, queue, ctas, threads, smem, st);
+        case 0: return launch_res_nb<0>(nt, P, sims, rules, results, queue, ring, ctas, threads, smem, st);
+        case 1: return launch_res_nb<1>(nt, P, sims, rules, results, queue, ring, ctas, threads, smem, st);
+        case 2: return launch_res_nb<2>(nt, P, sims, rules, results, queue, ring, ctas, threads, smem, st);
+        case 3: return launch_res_nb<3>(nt, P, sims, rules, results, queue, ring, ctas, threads, smem, st);
+        case 4: return launch_res_nb<4>(nt, P, sims, rules, results, queue, ring, ctas, threads, smem, st);
+        case 5: return launch_res_nb<5>(nt, P, sims, rules, results, queue, ring, ctas, threads, smem, st);
+        case 6: return launch_res_nb<6>(nt, P, sims, rules, results, queue, ring, ctas, threads, smem, st);
+        case 7: return launch_res_nb<7>(nt, P, sims, rules, results, queue, ring, ctas, threads, smem, st);
     }
     return cudaErrorInvalidValue;
 }

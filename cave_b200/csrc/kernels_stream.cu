@@ -25,11 +25,13 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <mutex>
 
 #include "ca_core.cuh"
 #include "cave_internal.h"
 #include "kernels.h"
 #include "ptx.cuh"
+#include "ring.cuh"
 
 namespace cave {
 
@@ -357,8 +359,26 @@ __device__ void fold_tick(StripSim* sim) {
         info.status = 0;
     sim->info = info;
     sim->tick = t + 1;
-    if ((sim->stop_on_status && info.status > 0) || t + 1 >= sim->tick_limit) sim->done = 1;
+    const bool done = (sim->stop_on_status && info.status > 0) || t + 1 >= sim->tick_limit;
+    if (done) sim->done = 1;
     __threadfence();
+    if (done && sim->ring) {
+        cave_sim_result r;
+        r.info = info;
+        r.category = result_category(info, sim->rule.maxcs);
+        r.tag = 0;
+        r.population = st.population;
+        r.activeTicks = sim->pop_change_ticks;
+        r.totalChanged = sim->total_changed;
+        for (int q = 0; q < 3; q++) {
+            r.bbox_min[q] = st.bbox_min[q];
+            r.bbox_max[q] = st.bbox_max[q];
+        }
+        r.params = cave_sim_params{0, 0, 0};
+        r.error = sim->error;
+        r.pad = 0;
+        ring_push(sim->ring, sim->slot, r);
+    }
 }
 
 
@@ -381,13 +401,17 @@ static bool stream_pdl() {
 template <int NB, int NT, bool PR>
 static cudaError_t launch_stream_inst(const StreamItem* items, uint32_t n_items, StripSim* sims, uint4* pool,
                                      uint32_t sxp_log2, uint32_t threads, size_t smem, const DeviceRule& rule,
-                                     cudaStream_t st) {
+                                     cudaStream_t st, bool pdl) {
     auto k = k_stream_tick<NB, NT, PR>;
-    static size_t configured = 0;
-    if (smem > configured) {
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        configured = smem;
+    static size_t configured = 0;  // largest dynamic shared memory set for this instance
+    static std::mutex mu;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (smem > configured) {
+            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            configured = smem;
+        }
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(n_items);
@@ -398,27 +422,27 @@ static cudaError_t launch_stream_inst(const StreamItem* items, uint32_t n_items,
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = stream_pdl() ? 1 : 0;
+    cfg.numAttrs = (pdl && stream_pdl()) ? 1 : 0;
     return cudaLaunchKernelEx(&cfg, k, items, sims, pool, sxp_log2, stream_pipe(), rule);
 }
 
 template <int NB, bool PR>
 static cudaError_t launch_stream_nt(int nt, const StreamItem* items, uint32_t n_items, StripSim* sims, uint4* pool,
                                    uint32_t sxp_log2, uint32_t threads, size_t smem, const DeviceRule& rule,
-                                   cudaStream_t st) {
+                                   cudaStream_t st, bool pdl) {
     switch (nt) {
-        case 0: return launch_stream_inst<NB, 0, PR>(items, n_items, sims, pool, sxp_log2, threads, smem, rule, st);
-        case 1: return launch_stream_inst<NB, 1, PR>(items, n_items, sims, pool, sxp_log2, threads, smem, rule, st);
-        case 2: return launch_stream_inst<NB, 2, PR>(items, n_items, sims, pool, sxp_log2, threads, smem, rule, st);
-        case 3: return launch_stream_inst<NB, 3, PR>(items, n_items, sims, pool, sxp_log2, threads, smem, rule, st);
-        case 4: return launch_stream_inst<NB, 4, PR>(items, n_items, sims, pool, sxp_log2, threads, smem, rule, st);
+        case 0: return launch_stream_inst<NB, 0, PR>(items, n_items, sims, pool, sxp_log2, threads, smem, rule, st, pdl);
+        case 1: return launch_stream_inst<NB, 1, PR>(items, n_items, sims, pool, sxp_log2, threads, smem, rule, st, pdl);
+        case 2: return launch_stream_inst<NB, 2, PR>(items, n_items, sims, pool, sxp_log2, threads, smem, rule, st, pdl);
+        case 3: return launch_stream_inst<NB, 3, PR>(items, n_items, sims, pool, sxp_log2, threads, smem, rule, st, pdl);
+        case 4: return launch_stream_inst<NB, 4, PR>(items, n_items, sims, pool, sxp_log2, threads, smem, rule, st, pdl);
         default: return cudaErrorInvalidValue;
     }
 }
 
 cudaError_t launch_stream_tick(int nb, int nt, const DeviceRule* param_rule, const StreamItem* items,
                                uint32_t n_items, StripSim* sims, uint4* pool, uint32_t SX, uint32_t SXp,
-                               uint32_t threads, cudaStream_t st) {
+                               uint32_t threads, cudaStream_t st, bool pdl) {
     uint32_t lg = 0;
     while ((1u << lg) < SXp) lg++;
     const uint32_t rows = threads / SXp;
@@ -427,8 +451,8 @@ cudaError_t launch_stream_tick(int nb, int nt, const DeviceRule* param_rule, con
     const DeviceRule& r = param_rule ? *param_rule : dummy;
 #define CAVE_NB_CASE(N)                                                                                        \
     case N:                                                                                                    \
-        return param_rule ? launch_stream_nt<N, true>(nt, items, n_items, sims, pool, lg, threads, smem, r, st) \
-                          : launch_stream_nt<N, false>(nt, items, n_items, sims, pool, lg, threads, smem, r, st);
+        return param_rule ? launch_stream_nt<N, true>(nt, items, n_items, sims, pool, lg, threads, smem, r, st, pdl) \
+                          : launch_stream_nt<N, false>(nt, items, n_items, sims, pool, lg, threads, smem, r, st, pdl);
     switch (nb & 7) {
         CAVE_NB_CASE(0)
         CAVE_NB_CASE(1)

@@ -272,22 +272,12 @@ static cave_status run_batched(cave_ctx* ctx, const cave_search_config& c, const
     }
     rc = cave_batch_add_sims(b, descs.data(), descs.size(), c.maxRuleBits);
     if (rc) return rc;
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventRecord(e0, ctx->stream);
     rc = cave_batch_launch(b);
-    cudaEventRecord(e1, ctx->stream);
     if (rc) return rc;
     std::vector<cave_sim_result> res(descs.size());
     rc = cave_batch_results(b, res.data(), res.size());
-    float ms = 0;
-    cudaEventSynchronize(e1);
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     if (rc) return rc;
-    dev_s = ms / 1e3;
+    dev_s = ctx->last_timing.tick_ms / 1e3;  // the batch's kernels, resident and tiled
     nsims = descs.size();
     per_chunk.assign(s.chunks.size(), {});
     for (size_t i = 0; i < res.size(); i++)

@@ -244,7 +244,29 @@ cave_status cave_batch_add_init_seeded(cave_batch* b, uint32_t X, uint32_t Y, ui
 cave_status cave_batch_add_table(cave_batch* b, const uint64_t* validBitmasks, uint32_t nValid, uint32_t* index);
 /* Queues simulations (maxRuleBits applies to all of them). */
 cave_status cave_batch_add_sims(cave_batch* b, const cave_sim_desc* sims, uint64_t n, uint32_t maxRuleBits);
-/* Starts every queued simulation on the device (non-blocking). */
+/* How a batch runs (set before cave_batch_launch; all-zero = defaults). Grids that fit one
+ * CTA's shared memory run on the resident kernel (one persistent launch per class, every tick
+ * on chip); larger grids run tiled: each keeps two bit-plane copies in HBM and every tick is a
+ * multi-CTA launch over all active simulations of its class, in rounds driven by a host
+ * worker thread, finished simulations leaving and waiting ones entering between rounds
+ * (searchMode.cpp:349-404 admits whole chunks against a VRAM budget instead). */
+typedef struct {
+    uint32_t autotune;       /* 1: time candidate executions (resident vs tiled, CTA size,
+                                CTAs per simulation) of each grid class once per context and
+                                keep the fastest; 0: defaults                                */
+    uint32_t tiledOnly;      /* 1: run every grid tiled (never resident)                       */
+    uint32_t ticksPerRound;  /* tiled: tick launches per class between scheduling steps (0 = 8) */
+    uint32_t pad;
+    uint64_t memoryBudget;   /* tiled: device bytes for grid copies (0 = half the free memory);
+                                a batch larger than this runs in waves                        */
+} cave_batch_options;
+cave_status cave_batch_set_options(cave_batch* b, const cave_batch_options* options);
+/* JSON array describing how each grid class of the last launch runs (path, tile shape);
+ * writes up to cap bytes (NUL-terminated) and returns the full length. */
+uint64_t cave_batch_plan(const cave_batch* b, char* out, uint64_t cap);
+
+/* Starts every queued simulation on the device (non-blocking). A context with a batch in
+ * flight should not be used for other calls until cave_batch_results has returned. */
 cave_status cave_batch_launch(cave_batch* b);
 /* Non-blocking completion poll (the IsTickComplete of searchSystem.cpp:467-478): CAVE_OK
  * when the launched work has finished, CAVE_ERR_NOT_READY otherwise. */
@@ -260,6 +282,67 @@ uint64_t cave_batch_size(const cave_batch* b);
  * Blocking. Results are identical to cave_batch_launch's; *deviceSeconds (may be NULL)
  * receives the device time of the tick loops. */
 cave_status cave_batch_run_plain(cave_batch* b, uint32_t slots, double* deviceSeconds);
+
+/* ---- serving: sweep requests admitted as they arrive -------------------------------------- */
+/* A server runs requests -- each a list of simulations, every one with its own grid, rule,
+ * tick limit and seeded initial cells -- on one GPU while more requests arrive. Simulations
+ * are admitted first-come first-served as slots and grid memory free up (continuous
+ * batching: a request that arrives while others run shares the GPU with them), grid state
+ * stays on the device between ticks, and a request completes when its last simulation has.
+ * Replaces SearchMode's chunk pool (searchMode.cpp:252-459; VRAM admission :349-404), which
+ * runs one sweep per process. Results are the same as a batch's for the same simulations. */
+typedef struct cave_server cave_server;
+
+/* One simulation of a request. The initial cells are the reference's seeding
+ * (searchSystem.cpp:219-306): a centred spawn box, a cell alive (state maxCellState) iff
+ * cellHash(x, y, z, runSeedIndex) < threshold (2^32 fills the box). */
+typedef struct {
+    uint32_t X, Y, Z;
+    uint32_t maxTicks;          /* MAX_NUMBER_OF_TICKS_TO_SURVIVE                         */
+    cave_sim_params params;     /* rule in bitmask form (no K-index)                      */
+    uint32_t spawnX, spawnY, spawnZ;
+    uint32_t runSeedIndex;
+    uint64_t threshold;
+    uint32_t tag;               /* caller's id, not interpreted                           */
+    uint32_t pad;
+} cave_request_sim;
+
+typedef struct {
+    uint64_t hbmBudget;         /* device bytes for grid state (0 = half the free memory)  */
+    uint32_t maxInFlight;       /* simulations on the device at once at most (0 = 16384)  */
+    uint32_t ticksPerRound;     /* tiled grids: tick launches per scheduling step (0 = 8)  */
+    uint32_t autotune;          /* as cave_batch_options                                   */
+    uint32_t tiledOnly;
+} cave_server_options;
+
+typedef struct {
+    uint64_t submitted, completed;      /* requests                                          */
+    uint64_t simsCompleted;
+    uint64_t cellUpdates;               /* ticks run x grid volume, finished simulations    */
+    double p50LatencySeconds;           /* submit -> last result, over completed requests   */
+    double p99LatencySeconds;
+    double busySeconds;                 /* wall time with at least one request outstanding  */
+    uint64_t peakBytes;                 /* largest grid memory in use                       */
+    uint64_t rounds, tickLaunches, residentLaunches;
+    double tuneMs;                      /* host time spent autotuning                       */
+} cave_server_stats;
+
+cave_status cave_server_create(cave_ctx* ctx, const cave_server_options* options, cave_server** out);
+/* Stops the scheduler and waits for device work in flight; unfetched results are dropped. */
+void cave_server_destroy(cave_server* s);
+/* Queues a request of n simulations (non-blocking) and returns its id. Fails with
+ * CAVE_ERR_OUT_OF_MEMORY when one simulation alone needs more than the budget. */
+cave_status cave_server_submit(cave_server* s, const cave_request_sim* sims, uint64_t n, uint64_t* requestId);
+/* Ids of requests that completed since the last poll (up to cap). Non-blocking. */
+cave_status cave_server_poll(cave_server* s, uint64_t* requestIds, uint64_t cap, uint64_t* n);
+/* Blocks until the request has completed (timeoutSeconds <= 0: no limit; CAVE_ERR_TIMEOUT
+ * when the time ran out). */
+cave_status cave_server_wait(cave_server* s, uint64_t requestId, double timeoutSeconds);
+/* Copies a completed request's results (n = its simulation count, submission order, params in
+ * the submitted form) and releases it; *latencySeconds = submit to completion. */
+cave_status cave_server_fetch(cave_server* s, uint64_t requestId, cave_sim_result* out, uint64_t n,
+                              double* latencySeconds);
+cave_status cave_server_get_stats(cave_server* s, cave_server_stats* out);
 
 /* ---- search sweeps (SearchMode + SearchSystem + RuleAggregator) ------------------------ */
 /* The search flags of the reference CLI (src/main.cpp:27-44, startupConfig.h) that shape a

@@ -1,0 +1,133 @@
+"""The request server (continuous batching): each request's results equal the oracle's and do
+not depend on what else is on the GPU -- alone, in a mix submitted while others run, and
+under an HBM budget small enough that simulations queue for memory. Integer work: exact."""
+import time
+
+import numpy as np
+import pytest
+
+import cave_b200 as cb
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def make_request(rng, n, edges=(24, 33, 40, 70, 100)):
+    r = cb.request_sims(n)
+    for i in range(n):
+        e = int(rng.choice(edges))
+        flags = int(rng.choice([1, 3, 7]))
+        nb = {1: 6, 3: 18, 7: 26}[flags]
+        maxcs = int(rng.integers(1, 16))
+        B = sum(1 << int(v) for v in rng.choice(nb, size=int(rng.integers(1, 5)), replace=False))
+        S = sum(1 << int(v) for v in rng.choice(nb, size=int(rng.integers(1, 5)), replace=False))
+        p = O.make_params(maxcs, flags, B, S)
+        r[i]["X"] = r[i]["Y"] = r[i]["Z"] = e
+        r[i]["maxTicks"] = int(rng.integers(1, 20))
+        r[i]["birth"], r[i]["survival"] = int(p[0]), int(p[1])
+        r[i]["spawnX"] = r[i]["spawnY"] = r[i]["spawnZ"] = e
+        r[i]["runSeedIndex"] = int(rng.integers(0, 1000))
+        r[i]["threshold"] = O.threshold_from_float(float(rng.uniform(0.2, 0.5)))
+        r[i]["tag"] = i
+    return r
+
+
+def oracle_result(sim):
+    X, Y, Z = int(sim["X"]), int(sim["Y"]), int(sim["Z"])
+    params = np.array([sim["birth"], sim["survival"], 0], dtype=np.uint64)
+    maxcs = int((int(sim["birth"]) >> 60) & 0xF) + 1
+    init = O.seed(X, Y, Z, spawn=(int(sim["spawnX"]),) * 3, random=True, threshold=int(sim["threshold"]),
+                  run_seed=int(sim["runSeedIndex"]), max_cell_state=maxcs)
+    info, ticks, _ = O.run_sim(X, Y, Z, params, init, int(sim["maxTicks"]), fast=True, per_tick=True)
+    last = ticks[-1]
+    return (info.as_tuple(), O.classify(info, maxcs), last.population, sum(t.changed for t in ticks),
+            sum(1 for t in ticks if t.changed), tuple(last.bbox_min), tuple(last.bbox_max))
+
+
+def as_tuple(r):
+    return (tuple(int(v) for v in r["info"]), int(r["category"]), int(r["population"]), int(r["totalChanged"]),
+            int(r["activeTicks"]), tuple(int(v) for v in r["bbox_min"]), tuple(int(v) for v in r["bbox_max"]))
+
+
+def run_alone(ctx, req, **kw):
+    with cb.Server(ctx, **kw) as s:
+        rid = s.submit(req)
+        assert s.wait(rid, 120.0)
+        res, lat = s.fetch(rid)
+    assert lat > 0
+    return res
+
+
+def test_request_matches_oracle(ctx):
+    rng = np.random.default_rng(3)
+    req = make_request(rng, 10)
+    res = run_alone(ctx, req, hbm_budget=1 << 30)
+    for i in range(req.size):
+        assert int(res[i]["error"]) == 0
+        assert as_tuple(res[i]) == oracle_result(req[i]), f"sim {i}"
+        assert int(res[i]["birth"]) == int(req[i]["birth"])
+
+
+def test_same_result_alone_and_in_mix(ctx):
+    rng = np.random.default_rng(17)
+    probe = make_request(rng, 12)
+    alone = run_alone(ctx, probe, hbm_budget=1 << 30)
+    others = [make_request(rng, int(rng.integers(1, 30))) for _ in range(6)]
+    with cb.Server(ctx, hbm_budget=1 << 30, ticks_per_round=2) as s:
+        ids = [s.submit(others[0]), s.submit(others[1])]
+        time.sleep(0.005)  # the probe arrives while the first requests are on the GPU
+        pid = s.submit(probe)
+        ids += [s.submit(o) for o in others[2:]]
+        for rid in ids + [pid]:
+            assert s.wait(rid, 300.0)
+        mixed, _ = s.fetch(pid)
+        outs = [s.fetch(rid)[0] for rid in ids]
+        st = s.stats()
+    for i in range(probe.size):
+        assert as_tuple(mixed[i]) == as_tuple(alone[i]), f"probe sim {i}"
+    # spot-check the other requests against the oracle
+    for o, r in zip(others[:2], outs[:2]):
+        for i in range(min(3, o.size)):
+            assert as_tuple(r[i]) == oracle_result(o[i])
+    assert st.completed == 7 and st.simsCompleted == probe.size + sum(o.size for o in others)
+    assert st.p99LatencySeconds >= st.p50LatencySeconds > 0
+
+
+def test_small_budget_queues_and_completes(ctx):
+    """Budget of a few 100^3 grids: simulations wait for memory, results stay exact."""
+    rng = np.random.default_rng(23)
+    req = make_request(rng, 16, edges=(100,))
+    alone = run_alone(ctx, req, hbm_budget=1 << 30)
+    per_sim = 2 * 4 * 100 * 100 * 16
+    with cb.Server(ctx, hbm_budget=3 * per_sim + (1 << 16), tiled_only=True) as s:
+        rid = s.submit(req)
+        assert s.wait(rid, 300.0)
+        res, _ = s.fetch(rid)
+        st = s.stats()
+    assert st.peakBytes <= 3 * per_sim + (1 << 16)
+    for i in range(req.size):
+        assert as_tuple(res[i]) == as_tuple(alone[i]), f"sim {i}"
+
+
+def test_oversized_simulation_is_rejected(ctx):
+    rng = np.random.default_rng(1)
+    req = make_request(rng, 1, edges=(100,))
+    with cb.Server(ctx, hbm_budget=1 << 16, tiled_only=True) as s:
+        with pytest.raises(cb.CaveError) as ei:
+            s.submit(req)
+        assert ei.value.code == cb.ERR_OUT_OF_MEMORY
+
+
+def test_poll_reports_each_request_once(ctx):
+    rng = np.random.default_rng(29)
+    reqs = [make_request(rng, 3, edges=(24, 33)) for _ in range(5)]
+    with cb.Server(ctx, hbm_budget=1 << 28) as s:
+        ids = [s.submit(r) for r in reqs]
+        seen = []
+        t0 = time.time()
+        while len(seen) < len(ids) and time.time() - t0 < 60:
+            seen += s.poll()
+            time.sleep(0.001)
+        for rid in ids:
+            s.fetch(rid)
+    assert sorted(seen) == sorted(ids)
