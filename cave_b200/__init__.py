@@ -139,7 +139,7 @@ class BatchOptions(ctypes.Structure):
 
 class ServerOptions(ctypes.Structure):
     _fields_ = [("hbmBudget", u64), ("maxInFlight", u32), ("ticksPerRound", u32), ("autotune", u32),
-                ("tiledOnly", u32)]
+                ("tiledOnly", u32), ("maxActiveCells", u64)]
 
 
 class ServerStats(ctypes.Structure):
@@ -512,9 +512,10 @@ class Server:
     """Sweep requests served as they arrive (cave_server): continuous batching on one GPU."""
 
     def __init__(self, ctx: Context, hbm_budget=0, max_in_flight=0, ticks_per_round=0, autotune=False,
-                 tiled_only=False):
+                 tiled_only=False, max_active_cells=0):
         self.ctx = ctx
-        o = ServerOptions(hbm_budget, max_in_flight, ticks_per_round, 1 if autotune else 0, 1 if tiled_only else 0)
+        o = ServerOptions(hbm_budget, max_in_flight, ticks_per_round, 1 if autotune else 0, 1 if tiled_only else 0,
+                          max_active_cells)
         h = ctypes.c_void_p()
         ctx.check(lib().cave_server_create(ctx.h, ctypes.byref(o), ctypes.byref(h)), "cave_server_create")
         self.h = h

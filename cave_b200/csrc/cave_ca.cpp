@@ -114,10 +114,11 @@ bool plan_stream(uint32_t sim_index, uint32_t X, uint32_t Y, uint32_t Z, uint32_
             it.ty = (uint16_t)std::min(ty, Y - iy * ty);
             it.z0 = (uint16_t)(iz * slab);
             it.z1 = (uint16_t)std::min(Z, (iz + 1) * slab);
-            it.dir = iz & 1u;
+            it.dir_items = iz & 1u;
             plan.items.push_back(it);
         }
     }
+    for (StreamItem& it : plan.items) it.dir_items |= (uint32_t)plan.items.size() << 1;
     return true;
 }
 
@@ -173,6 +174,11 @@ void cave_ctx_destroy(cave_ctx* ctx) {
     }
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
+    for (const cave::StagingPair& sp : ctx->staging_free)
+        for (int i = 0; i < 2; i++) {
+            cudaFreeHost(sp.h[i]);
+            cudaFree(sp.d[i]);
+        }
     delete ctx;
 }
 

@@ -10,8 +10,8 @@ namespace cave {
 
 constexpr uint64_t kPermMask = (uint64_t(1) << 60) - 1;  // simulation.h:43
 
-// Bounded device-side waits give up after this many polls and raise an error flag.
-constexpr uint32_t kSpinLimit = 1u << 26;
+// Bounded device-side waits give up after this many nanoseconds and raise an error flag.
+constexpr uint64_t kWaitLimitNs = 1000000000ull;
 
 // Error flags a kernel may raise in its record (read back by the host).
 enum : uint32_t { kErrNone = 0, kErrWaitTimeout = 1, kErrBadRuleIndex = 2 };
@@ -108,7 +108,8 @@ struct StripSim {
     uint32_t max_ticks;         // MAX_NUMBER_OF_TICKS_TO_SURVIVE
     uint32_t tick_limit;        // ticks to run in total (raw stepping) or max_ticks (search)
     uint32_t stop_on_status;    // 1: stop when the manager reports status > 0
-    uint32_t n_items;           // CTAs (work items) per tick for this simulation
+    uint32_t n_items;           // work items per tick when the record was written (the kernel
+                                // takes the count from each item, so launches may re-tile)
     uint32_t tick;              // ticks completed
     uint32_t done;              // no further ticks run
     uint32_t error;

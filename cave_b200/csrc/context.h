@@ -32,6 +32,12 @@ struct TuneKey {
         return nb < o.nb;
     }
 };
+// Pinned host staging plus its device mirror, two of each (the engine's upload buffers).
+struct StagingPair {
+    unsigned char* h[2];
+    unsigned char* d[2];
+    uint64_t cap;
+};
 }  // namespace cave
 
 struct cave_ctx {
@@ -46,6 +52,9 @@ struct cave_ctx {
     // autotuner results, shared by every batch and server of the context
     std::mutex tune_mu;
     std::map<cave::TuneKey, cave::ExecChoice> tune_cache;
+    // engine staging buffers released by finished engines, reused by the next (freed with the context)
+    std::mutex staging_mu;
+    std::vector<cave::StagingPair> staging_free;
 };
 
 struct cave_grid {

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <thread>
@@ -85,6 +86,9 @@ struct Engine::Slot {
     uint64_t mem_off = 0, mem_bytes = 0;  // cell memory in the pool (0 bytes: none)
     uint64_t volume = 0;
     TiledClass* cls = nullptr;
+    // tiled: grid, the class's rows per CTA, the preferred and the current CTAs per tick
+    uint32_t X = 0, Y = 0, Z = 0, rows_hint = 0;
+    uint32_t pref_ctas = 0, cur_ctas = 0;
     std::vector<StreamItem> items;
 };
 
@@ -120,13 +124,18 @@ Engine::~Engine() {
     cudaFree(desc_);
     cudaFree(recs_);
     cudaFree(ring_);
-    for (int i = 0; i < 2; i++) {
-        cudaFreeHost(stage_h_[i]);
-        cudaFree(stage_d_[i]);
+    if (stage_cap_) {  // keep the pinned staging for the context's next engine
+        std::lock_guard<std::mutex> lock(ctx_->staging_mu);
+        ctx_->staging_free.push_back(StagingPair{{stage_h_[0], stage_h_[1]}, {stage_d_[0], stage_d_[1]}, stage_cap_});
     }
     cudaFreeHost(host_entries_);
     if (ev_first_) cudaEventDestroy(ev_first_);
     if (ev_last_) cudaEventDestroy(ev_last_);
+    if (trace_) fclose(trace_);
+}
+
+double Engine::trace_us() const {
+    return std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - trace_t0_).count();
 }
 
 cave_status Engine::init(const EngineConfig& cfg) {
@@ -165,6 +174,22 @@ cave_status Engine::init(const EngineConfig& cfg) {
     for (uint32_t i = cfg_.max_slots; i-- > 0;) free_slots_.push_back(i);
     CAVE_CUDA(ctx_, cudaEventCreate(&ev_first_));
     CAVE_CUDA(ctx_, cudaEventCreate(&ev_last_));
+    {  // reuse pinned staging left by an earlier engine of this context (page-locking is slow)
+        std::lock_guard<std::mutex> lock(ctx_->staging_mu);
+        if (!ctx_->staging_free.empty()) {
+            const StagingPair sp = ctx_->staging_free.back();
+            ctx_->staging_free.pop_back();
+            for (int i = 0; i < 2; i++) {
+                stage_h_[i] = sp.h[i];
+                stage_d_[i] = sp.d[i];
+            }
+            stage_cap_ = sp.cap;
+        }
+    }
+    if (const char* path = std::getenv("CAVE_ENGINE_TRACE")) {
+        trace_ = std::fopen(path, "a");
+        trace_t0_ = std::chrono::steady_clock::now();
+    }
     ready_ = true;
     return CAVE_OK;
 }
@@ -315,7 +340,8 @@ ExecChoice Engine::choose(const EngineSim& s) {
 // trials run once per class and context).
 cave_status tune_class(cave_ctx* ctx, cudaStream_t st, const EngineSim& s, bool tiled_only, ExecChoice& out) {
     constexpr uint32_t kTrialTicks = 4;
-    constexpr uint32_t kMaxRep = 64;
+    constexpr uint32_t kMaxRep = 64;         // resident replicas (one wave at most)
+    constexpr uint64_t kMaxTiledRep = 256;   // tiled replicas
     const uint32_t sms = (uint32_t)ctx->sm_count;
     const uint64_t strips = grid_strips(s.X, s.Y, s.Z);
     const uint64_t grid_bytes = strips * 16;
@@ -344,9 +370,16 @@ cave_status tune_class(cave_ctx* ctx, cudaStream_t st, const EngineSim& s, bool 
             cands.push_back(t);
         }
     }
-    const uint32_t reps_tiled = (uint32_t)std::min<uint64_t>(
-        kMaxRep, std::max<uint64_t>(1, (2ull * sms + p0.items.size() - 1) / p0.items.size()));
+    // Tiled candidates all run the same replicas: enough that the candidate with the fewest
+    // CTAs per grid still has about four waves of CTAs (two per SM per wave), within 2 GB.
     const uint64_t tiled_bytes = align_up(2 * grid_bytes, 256);
+    uint64_t fewest = p0.items.size();
+    for (const ExecChoice& c : cands) {
+        StreamPlan p;
+        if (!c.resident && plan_tiled(0, s.X, s.Y, s.Z, c, p)) fewest = std::min<uint64_t>(fewest, p.items.size());
+    }
+    const uint32_t reps_tiled = (uint32_t)std::max<uint64_t>(
+        1, std::min<uint64_t>({kMaxTiledRep, (8ull * sms + fewest - 1) / fewest, (2ull << 30) / tiled_bytes}));
     const uint64_t init_bytes = align_up(grid_bytes, 256);
     const uint64_t desc_bytes = desc_bytes_for(kMaxRep);
     unsigned char* base = nullptr;
@@ -354,9 +387,9 @@ cave_status tune_class(cave_ctx* ctx, cudaStream_t st, const EngineSim& s, bool 
     StreamItem* titems = nullptr;
     cave_sim_result* tres = nullptr;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
-    constexpr uint32_t kMaxItems = 1u << 16;
+    constexpr uint32_t kMaxItems = 1u << 18;
     cudaError_t e = cudaMalloc(&base, init_bytes + desc_bytes + reps_tiled * tiled_bytes);
-    if (e == cudaSuccess) e = cudaMalloc(&trecs, sizeof(StripSim) * kMaxRep);
+    if (e == cudaSuccess) e = cudaMalloc(&trecs, sizeof(StripSim) * reps_tiled);
     if (e == cudaSuccess) e = cudaMalloc(&titems, sizeof(StreamItem) * kMaxItems);
     if (e == cudaSuccess) e = cudaMalloc(&tres, sizeof(cave_sim_result) * kMaxRep);
     if (e == cudaSuccess) e = cudaEventCreate(&t0);
@@ -481,6 +514,7 @@ cave_status Engine::consume_ring(bool* any) {
         if (slot >= slots_.size() || !slots_[slot])
             return set_error(ctx_, CAVE_ERR_INTERNAL, "engine: completion for an unknown slot");
         Slot* s = slots_[slot];
+        active_cells_ -= s->volume;
         if (s->mem_bytes) cells_.free(s->mem_off, s->mem_bytes);
         if (s->cls) {
             auto& v = s->cls->slots;
@@ -502,7 +536,9 @@ cave_status Engine::consume_ring(bool* any) {
 cave_status Engine::retire(bool block) {
     while (!rounds_.empty()) {
         Round* r = rounds_.front();
+        const double w0 = (trace_ && block) ? trace_us() : 0;
         const cudaError_t q = block ? cudaEventSynchronize(r->done) : cudaEventQuery(r->done);
+        if (trace_ && block) std::fprintf(trace_, "{\"ev\":\"wait\",\"t_us\":%.1f,\"us\":%.1f}\n", w0, trace_us() - w0);
         if (q == cudaErrorNotReady) break;
         if (q != cudaSuccess) return check_cuda(ctx_, q, "engine round");
         cudaEventDestroy(r->done);
@@ -536,6 +572,8 @@ cave_status Engine::admit(std::vector<EngineSim>& admitted) {
     }
     while (!pending_.empty() && !free_slots_.empty()) {
         EngineSim& s = pending_.front();
+        const uint64_t vol = (uint64_t)s.X * s.Y * s.Z;
+        if (cfg_.max_active_cells && active_cells_ && active_cells_ + vol > cfg_.max_active_cells) break;
         const ExecChoice c = choose(s);
         const uint64_t strips = grid_strips(s.X, s.Y, s.Z);
         uint64_t bytes = c.resident ? (s.init ? 0 : strips * 16) : 2 * strips * 16;
@@ -548,10 +586,16 @@ cave_status Engine::admit(std::vector<EngineSim>& admitted) {
         sl->resident = c.resident;
         sl->mem_off = off;
         sl->mem_bytes = bytes;
-        sl->volume = (uint64_t)s.X * s.Y * s.Z;
+        sl->volume = vol;
+        active_cells_ += vol;
         if (!c.resident) {
             StreamPlan p;
             plan_tiled(slot, s.X, s.Y, s.Z, c, p);
+            sl->X = s.X;
+            sl->Y = s.Y;
+            sl->Z = s.Z;
+            sl->rows_hint = c.rows;
+            sl->pref_ctas = sl->cur_ctas = (uint32_t)p.items.size();
             sl->items = std::move(p.items);
             const auto ck = std::make_tuple(p.SXp, s.nb, s.nt, p.rows);
             TiledClass*& cls = classes_[ck];
@@ -581,6 +625,30 @@ cave_status Engine::admit(std::vector<EngineSim>& admitted) {
 
 cave_status Engine::launch_round(std::vector<EngineSim>& admitted) {
     const int b = (int)(round_no_ & 1u);
+    const double trace_start = trace_ ? trace_us() : 0;
+    // ---- tiling for this round: each simulation's preferred CTA count (its class's cells
+    // per CTA), scaled up when all active tiled simulations together would give fewer than
+    // two CTAs per SM (the tail of a batch), down to 2^14 cells per CTA
+    {
+        uint64_t pref = 0;
+        for (auto& kv : classes_)
+            for (uint32_t sl : kv.second->slots) pref += slots_[sl]->pref_ctas;
+        const uint64_t want = 2ull * (uint64_t)ctx_->sm_count;
+        for (auto& kv : classes_)
+            for (uint32_t sl : kv.second->slots) {
+                Slot* s = slots_[sl];
+                uint64_t t = s->pref_ctas;
+                if (pref && pref < want)
+                    t = std::min<uint64_t>((t * want + pref - 1) / pref, std::max<uint64_t>(t, s->volume >> 14));
+                if (t != s->cur_ctas) {
+                    StreamPlan p;
+                    if (plan_stream(sl, s->X, s->Y, s->Z, (uint32_t)t, s->rows_hint, p) && p.rows == kv.second->rows) {
+                        s->items = std::move(p.items);
+                        s->cur_ctas = (uint32_t)t;
+                    }
+                }
+            }
+    }
     // ---- staging layout
     size_t n_items = 0;
     for (auto& kv : classes_)
@@ -617,7 +685,7 @@ cave_status Engine::launch_round(std::vector<EngineSim>& admitted) {
             if (cave_status rc = retire(true); rc) return rc;
         CAVE_CUDA(ctx_, cudaStreamSynchronize(copy_));
         CAVE_CUDA(ctx_, cudaStreamSynchronize(main_));
-        const uint64_t cap = std::max<uint64_t>(total * 2, 1u << 20);
+        const uint64_t cap = std::max<uint64_t>(total * 2, 4u << 20);
         for (int i = 0; i < 2; i++) {
             cudaFreeHost(stage_h_[i]);
             cudaFree(stage_d_[i]);
@@ -809,6 +877,16 @@ cave_status Engine::launch_round(std::vector<EngineSim>& admitted) {
     {
         std::lock_guard<std::mutex> lock(mu_);
         stats_.rounds++;
+    }
+    if (trace_) {
+        size_t active = 0;
+        for (auto& kv : classes_) active += kv.second->slots.size();
+        std::fprintf(trace_,
+                     "{\"ev\":\"round\",\"no\":%llu,\"t_us\":%.1f,\"enqueue_us\":%.1f,\"admitted\":%zu,"
+                     "\"tiled_active\":%zu,\"classes\":%zu,\"items\":%zu,\"resident_launches\":%zu,"
+                     "\"pool_bytes\":%llu}\n",
+                     (unsigned long long)round_no_, trace_start, trace_us() - trace_start, admitted.size(), active,
+                     cl.size(), ni, launches.size(), (unsigned long long)cells_.used());
     }
     if (e != cudaSuccess) return check_cuda(ctx_, e, "engine round");
     return CAVE_OK;

@@ -23,6 +23,8 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <chrono>
+#include <cstdio>
 #include <condition_variable>
 #include <cstdint>
 #include <deque>
@@ -71,6 +73,8 @@ struct EngineConfig {
     uint32_t ticks_per_round = 8;    // tick launches per class per round
     uint32_t tiled_only = 0;         // 1: never use the resident kernel
     uint32_t autotune = 0;           // 1: time candidate choices for unseen classes
+    uint64_t max_active_cells = 0;   // admission stops while admitted grids hold this many
+                                     // cells (0: no limit besides memory and slots)
 };
 
 struct EngineResult {
@@ -163,6 +167,7 @@ private:
     std::deque<Round*> rounds_;      // in flight, oldest first
     std::vector<ResGroup*> groups_;  // resident launches in flight
     uint64_t round_no_ = 0;
+    uint64_t active_cells_ = 0;      // grid volume of the admitted, unfinished simulations
     uint32_t res_rr_ = 0;
     // queues
     std::mutex mu_;
@@ -173,6 +178,10 @@ private:
     cudaEvent_t ev_first_ = nullptr, ev_last_ = nullptr;
     bool first_recorded_ = false;
     std::map<TuneKey, ExecChoice> plan_used_;
+    // optional scheduling trace (JSON lines): path from the CAVE_ENGINE_TRACE environment variable
+    FILE* trace_ = nullptr;
+    std::chrono::steady_clock::time_point trace_t0_;
+    double trace_us() const;
 };
 
 }  // namespace cave

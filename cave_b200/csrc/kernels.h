@@ -23,7 +23,8 @@ struct StreamItem {
     uint32_t sim;            // index into the StripSim array
     uint16_t y0, ty;         // output rows [y0, y0 + ty)
     uint16_t z0, z1;         // output planes [z0, z1)
-    uint32_t dir;            // 0: march towards +z, 1: towards -z
+    uint32_t dir_items;      // bit 0: march towards +z (0) or -z (1); bits 1..31: the number of
+                             // work items of `sim` in this launch (the last one to finish folds)
 };
 
 cudaError_t launch_plain_step(const uint32_t* in, uint32_t* out, uint32_t X, uint32_t Y, uint32_t Z,

@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(1024) k_resident(ResLaunch P, const ResSim* __
             bulk_g2s(grid, sd.init, grid_bytes, &s_bar);
         }
         uint32_t err = 0;
-        if (!mbar_wait_bounded(&s_bar, bar_phase, kSpinLimit)) err = kErrWaitTimeout;
+        if (!mbar_wait_bounded(&s_bar, bar_phase, kWaitLimitNs)) err = kErrWaitTimeout;
         bar_phase ^= 1u;
         __syncthreads();  // rule visible
         DeviceRule R;

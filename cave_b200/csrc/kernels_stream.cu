@@ -116,21 +116,28 @@ __global__ void __launch_bounds__(1024) k_stream_tick(const StreamItem* __restri
     const uint32_t slot_stride = rows * SX;
     const int L = (int)it.z1 - (int)it.z0;  // output planes
     const int nfetch = L + 2;
-    const int zstep = it.dir ? -1 : 1;
-    const int zfirst = it.dir ? (int)it.z1 : (int)it.z0 - 1;  // plane of fetch 0
+    const bool down = (it.dir_items & 1u) != 0;
+    const int zstep = down ? -1 : 1;
+    const int zfirst = down ? (int)it.z1 : (int)it.z0 - 1;  // plane of fetch 0
 
-    auto issue = [&](int f) {
+    // Thread 0 fills ring slot f % kRing with input plane f. A plane outside the grid is not
+    // copied; with `complete` set its slot's phase is completed by a plain arrive, so that every
+    // fetch advances its slot by exactly one phase (the grouped march relies on that).
+    auto issue = [&](int f, bool complete = false) {
         if (f >= nfetch) return;
         const int p = zfirst + f * zstep;
-        if (p < 0 || p >= (int)Z) return;
         const int s = f & (kRing - 1);
+        if (p < 0 || p >= (int)Z) {
+            if (complete) mbar_arrive(&bars[s]);
+            return;
+        }
         uint4* slot = ring + (size_t)s * slot_stride + (size_t)slot_row0 * SX;
         const uint4* g = src + ((size_t)p * Y + (size_t)ylo) * SX;
         mbar_expect_tx(&bars[s], tile_bytes);
         bulk_g2s(slot, g, tile_bytes, &bars[s]);
     };
     if (threadIdx.x == 0) {
-        for (int f = 0; f < kRing; f++) issue(f);
+        for (int f = 0; f < kRing; f++) issue(f, pipe == 2);
     }
 
     const uint4* my_ring = ring + (size_t)yy * SX + sx;
@@ -140,7 +147,7 @@ __global__ void __launch_bounds__(1024) k_stream_tick(const StreamItem* __restri
         const int p = zfirst + f * zstep;
         if (p < 0 || p >= (int)Z) return make_uint4(0, 0, 0, 0);
         const int s = f & (kRing - 1);
-        if (!mbar_wait_bounded(&bars[s], (phase >> s) & 1u, kSpinLimit)) err = kErrWaitTimeout;
+        if (!mbar_wait_bounded(&bars[s], (phase >> s) & 1u, kWaitLimitNs)) err = kErrWaitTimeout;
         phase ^= 1u << s;
         return has ? my_ring[(size_t)s * slot_stride] : make_uint4(0, 0, 0, 0);
     };
@@ -163,7 +170,59 @@ __global__ void __launch_bounds__(1024) k_stream_tick(const StreamItem* __restri
     const size_t xpar = (size_t)rows * SXp;
 
     int zo = zfirst + zstep;
-    if (!pipe) {
+    if (pipe == 2) {
+        // Grouped order: the plain order below, unrolled by the ring size so that ring slots
+        // and exchange buffers are compile-time constants and the plane rotation needs no
+        // register moves. Every warp waits for the copy of the plane it reads; fetch f is the
+        // (f / kRing)-th use of slot f % kRing, so the phase parity to wait for is (f / kRing) & 1.
+        auto read = [&](int f, int s) -> uint4 {  // s == f % kRing
+            const int p = zfirst + f * zstep;
+            if (f >= nfetch || (unsigned)p >= Z) return make_uint4(0, 0, 0, 0);
+            if (!mbar_wait_bounded(&bars[s], (uint32_t)(f >> 2) & 1u, kWaitLimitNs)) err = kErrWaitTimeout;
+            return has ? my_ring[(size_t)s * slot_stride] : make_uint4(0, 0, 0, 0);
+        };
+        Row r_m = row_of(read(0, 0));
+        uint4 s_c = read(1, 1);
+        Row r_c = row_of(s_c);
+        __syncthreads();  // slots 0 and 1 consumed
+        if (threadIdx.x == 0) {
+            fence_proxy_async();
+            issue(kRing, true);
+            issue(kRing + 1, true);
+        }
+        auto body = [&]<int U>(int k) {  // k % kRing == U
+            const uint4 s_in = read(k + 2, (U + 2) & (kRing - 1));
+            const Row r_p = row_of(s_in);
+            uint32_t pc[P::NC], ps[P::NS];
+            P::make(r_m, r_c, r_p, pc, ps);
+            uint4* xb = my_x + (size_t)(U & 1) * xpar;
+            *xb = pack_planes<P::NS>(ps);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                fence_proxy_async();
+                issue(k + 2 + kRing, true);
+            }
+            if (outp) {
+                const uint4 qm = *(xb - SXp), qp = *(xb + SXp);
+                const uint32_t psm[4] = {qm.x, qm.y, qm.z, qm.w}, psp[4] = {qp.x, qp.y, qp.z, qp.w};
+                uint32_t cnt[count_bits(NB)];
+                combine<NB>(pc, psm, psp, cnt);
+                my_dst[(size_t)zo * plane_stride] =
+                    update_strip<NB, NT>(s_c, r_c.a, cnt, valid, R, acc, xbits, (uint32_t)zo);
+            }
+            r_m = r_c;
+            r_c = r_p;
+            s_c = s_in;
+            zo += zstep;
+        };
+        static_assert(kRing == 4, "the grouped march is unrolled by the ring size");
+        for (int k = 0; k < L; k += kRing) {
+            body.template operator()<0>(k);
+            if (k + 1 < L) body.template operator()<1>(k + 1);
+            if (k + 2 < L) body.template operator()<2>(k + 2);
+            if (k + 3 < L) body.template operator()<3>(k + 3);
+        }
+    } else if (!pipe) {
         // Plain order: per plane, column sums -> barrier -> count, rule, update, store.
         Row r_m = row_of(fetch(0));
         uint4 s_c = fetch(1);
@@ -308,7 +367,7 @@ __global__ void __launch_bounds__(1024) k_stream_tick(const StreamItem* __restri
         }
         if (red[0][10]) atomicOr(&sim->error, red[0][10]);
         __threadfence();
-        s_last = atomicAdd(&sim->ticket, 1u) == sim->n_items - 1u;
+        s_last = atomicAdd(&sim->ticket, 1u) == (it.dir_items >> 1) - 1u;
     }
     __syncthreads();
     if (threadIdx.x == 0 && s_last) {
@@ -384,14 +443,15 @@ __device__ void fold_tick(StripSim* sim) {
 
 
 // ------------------------------------------------------------------ launch helpers
-// Variant switches for tuning runs: CAVE_STREAM_PIPE (software-pipelined march, default 0)
-// and CAVE_STREAM_PDL (programmatic dependent launch between ticks, default 1).
+// Variant switches for tuning runs: CAVE_STREAM_PIPE (march order: 2 grouped, the default;
+// 0 plain; 1 software-pipelined) and CAVE_STREAM_PDL (programmatic dependent launch between
+// ticks, default 1).
 static uint32_t env_flag(const char* name, uint32_t dflt) {
     const char* v = std::getenv(name);
     return v ? (uint32_t)std::atoi(v) : dflt;
 }
 static uint32_t stream_pipe() {
-    static const uint32_t v = env_flag("CAVE_STREAM_PIPE", 0);
+    static const uint32_t v = env_flag("CAVE_STREAM_PIPE", 2);
     return v;
 }
 static bool stream_pdl() {

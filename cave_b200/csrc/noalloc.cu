@@ -77,7 +77,7 @@ __global__ void k_noalloc_setup(StripSim rec, StripSim* dst, StreamItem* items, 
         it.ty = (uint16_t)min(ty, Y - iy * ty);
         it.z0 = (uint16_t)(iz * slab);
         it.z1 = (uint16_t)min(Z, (iz + 1) * slab);
-        it.dir = iz & 1u;
+        it.dir_items = (n << 1) | (iz & 1u);
         items[i] = it;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) *dst = rec;

@@ -30,11 +30,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Waits for phase `parity` of `bar`, giving up after `limit` polls (returns false then).
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t limit) {
-    uint32_t spins = 0;
+// Nanoseconds of the GPU's global timer.
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Waits for phase `parity` of `bar`, giving up after `limit_ns` nanoseconds (returns false
+// then). The first poll needs no timer read.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
     while (!mbar_try_wait(bar, parity)) {
-        if (++spins > limit) return false;
+        if (global_ns() - t0 > limit_ns) return false;
     }
     return true;
 }

@@ -131,6 +131,7 @@ cave_status cave_server_create(cave_ctx* ctx, const cave_server_options* opt, ca
     ec.ticks_per_round = o.ticksPerRound ? o.ticksPerRound : 8u;
     ec.tiled_only = o.tiledOnly;
     ec.autotune = o.autotune;
+    ec.max_active_cells = o.maxActiveCells ? o.maxActiveCells : (1ull << 31);
     s->engine = std::make_unique<Engine>(ctx);
     const cave_status rc = s->engine->init(ec);
     if (rc) {

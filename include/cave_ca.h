@@ -313,6 +313,10 @@ typedef struct {
     uint32_t ticksPerRound;     /* tiled grids: tick launches per scheduling step (0 = 8)  */
     uint32_t autotune;          /* as cave_batch_options                                   */
     uint32_t tiledOnly;
+    uint64_t maxActiveCells;    /* admission pauses while the admitted grids hold this many
+                                   cells (0 = 2^31, several ticks of work for the GPU): the
+                                   oldest requests run first instead of every request
+                                   sharing the GPU; ~0 = limited by memory only            */
 } cave_server_options;
 
 typedef struct {

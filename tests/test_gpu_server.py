@@ -109,6 +109,16 @@ def test_small_budget_queues_and_completes(ctx):
         assert as_tuple(res[i]) == as_tuple(alone[i]), f"sim {i}"
 
 
+def test_one_at_a_time_admission_gives_same_results(ctx):
+    """An active-cell cap of one cell admits a single simulation at a time (FIFO)."""
+    rng = np.random.default_rng(31)
+    req = make_request(rng, 6)
+    alone = run_alone(ctx, req, hbm_budget=1 << 30)
+    capped = run_alone(ctx, req, hbm_budget=1 << 30, max_active_cells=1)
+    for i in range(req.size):
+        assert as_tuple(capped[i]) == as_tuple(alone[i]), f"sim {i}"
+
+
 def test_oversized_simulation_is_rejected(ctx):
     rng = np.random.default_rng(1)
     req = make_request(rng, 1, edges=(100,))
