@@ -159,24 +159,24 @@ def barrier(pg, local):
     torch.cuda.synchronize(local)
 
 
-def max_over_ranks(pg, local, v):
+def _reduce(pg, local, v, op):
+    """All-reduce of one float over the ranks (no-op without a process group). local = None
+    reduces on the CPU (gloo), else on cuda:local (nccl)."""
     if not pg:
         return v
     import torch
 
-    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    t = torch.tensor([v], dtype=torch.float64, device="cpu" if local is None else f"cuda:{local}")
+    pg.all_reduce(t, op=op)
     return float(t.item())
+
+
+def max_over_ranks(pg, local, v):
+    return _reduce(pg, local, v, pg.ReduceOp.MAX if pg else None)
 
 
 def sum_over_ranks(pg, local, v):
-    if not pg:
-        return v
-    import torch
-
-    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
-    pg.all_reduce(t, op=pg.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(pg, local, v, pg.ReduceOp.SUM if pg else None)
 
 
 # ----------------------------------------------------------------------------- CPU baseline

@@ -213,6 +213,10 @@ _SIGS = {
     "cave_server_wait": (i32, [ctypes.c_void_p, u64, ctypes.c_double]),
     "cave_server_fetch": (i32, [ctypes.c_void_p, u64, ctypes.c_void_p, u64, P(ctypes.c_double)]),
     "cave_server_get_stats": (i32, [ctypes.c_void_p, P(ServerStats)]),
+    "cave_render_buffer_elements": (u64, [u32, u32, u32]),
+    "cave_render_skip_elements": (u64, [u32, u32, u32]),
+    "cave_render_step": (i32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, u32, u32, u32, P(SimParams), u32,
+                               ctypes.c_void_p]),
     "cave_search_run": (i32, [ctypes.c_void_p, P(SearchConfig), u32, u64, P(SearchSummary)]),
     "cave_rule_string_to_bitmask": (u64, [ctypes.c_char_p]),
     "cave_bitmask_to_rule_string": (u64, [u64, ctypes.c_char_p, u64]),
@@ -392,6 +396,20 @@ def run_noalloc(ctx: Context, in_ptr, out_ptr, X, Y, Z, params: SimParams, ntick
                                      nticks, nticks if max_ticks is None else max_ticks,
                                      ctypes.c_void_p(per_tick_ptr or 0), ctypes.byref(info)), "cave_run_noalloc")
     return info
+
+
+def render_buffer_elements(X, Y, Z) -> int:
+    return int(lib().cave_render_buffer_elements(X, Y, Z))
+
+
+def render_skip_elements(X, Y, Z) -> int:
+    return int(lib().cave_render_skip_elements(X, Y, Z))
+
+
+def render_step(ctx: Context, in_ptr, out_ptr, X, Y, Z, params: SimParams, nticks=1, skip_ptr=None):
+    """cave_render_step on device buffers (addresses as ints) in the render mode's layout."""
+    ctx.check(lib().cave_render_step(ctx.h, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr), X, Y, Z,
+                                     ctypes.byref(params), nticks, ctypes.c_void_p(skip_ptr or 0)), "cave_render_step")
 
 
 def search_run(ctx: Context, config: SearchConfig, plain=False, sim_limit=0) -> SearchSummary:

@@ -340,7 +340,7 @@ ExecChoice Engine::choose(const EngineSim& s) {
 // trials run once per class and context).
 cave_status tune_class(cave_ctx* ctx, cudaStream_t st, const EngineSim& s, bool tiled_only, ExecChoice& out) {
     constexpr uint32_t kTrialTicks = 4;
-    constexpr uint32_t kMaxRep = 64;         // resident replicas (one wave at most)
+    constexpr uint32_t kMaxRep = 1024;       // resident replicas (one wave: SMs x CTAs per SM)
     constexpr uint64_t kMaxTiledRep = 256;   // tiled replicas
     const uint32_t sms = (uint32_t)ctx->sm_count;
     const uint64_t strips = grid_strips(s.X, s.Y, s.Z);
@@ -403,12 +403,13 @@ cave_status tune_class(cave_ctx* ctx, cudaStream_t st, const EngineSim& s, bool 
         else
             e = launch_seed_strips(init, s.seed, st);
     }
-    double best = -1;
-    ExecChoice best_c = cands[0];
-    for (size_t ci = 0; ci < cands.size() && e == cudaSuccess; ci++) {
-        const ExecChoice& c = cands[ci];
-        uint64_t updates = 0;
-        float ms = 0;
+    // Each candidate runs twice, for kTrialTicks and 3 * kTrialTicks ticks; the rate compared is
+    // the marginal one, (updates difference) / (time difference), so that one-off costs (the
+    // resident kernel loading a whole grid into shared memory, the first launch) do not count
+    // against a candidate in runs of hundreds of ticks.
+    auto run = [&](const ExecChoice& c, uint32_t T, uint64_t& updates, float& ms) {
+        updates = 0;
+        ms = 0;
         if (c.resident) {
             uint32_t threads = 0;
             ResLaunch P = resident_geometry(s.X, s.Y, s.Z, c.nseg, threads);
@@ -416,7 +417,7 @@ cave_status tune_class(cave_ctx* ctx, cudaStream_t st, const EngineSim& s, bool 
             const uint32_t n = std::min<uint32_t>(kMaxRep, sms * per_sm);
             P.n_sims = n;
             std::vector<ResSim> rs(n);
-            for (uint32_t i = 0; i < n; i++) rs[i] = ResSim{init, 0u, kTrialTicks, i, 0u};
+            for (uint32_t i = 0; i < n; i++) rs[i] = ResSim{init, 0u, T, i, 0u};
             uint32_t* queue = reinterpret_cast<uint32_t*>(desc);
             ResSim* dsims = reinterpret_cast<ResSim*>(desc + 16);
             DeviceRule* drule = reinterpret_cast<DeviceRule*>(desc + desc_rules_offset(kMaxRep));
@@ -431,7 +432,7 @@ cave_status tune_class(cave_ctx* ctx, cudaStream_t st, const EngineSim& s, bool 
             if (e == cudaSuccess)
                 e = cudaMemcpyAsync(hr.data(), tres, sizeof(cave_sim_result) * n, cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-            if (e != cudaSuccess) break;
+            if (e != cudaSuccess) return;
             cudaEventElapsedTime(&ms, t0, t1);
             for (const auto& r : hr) updates += (uint64_t)r.info.numberOfSimulationTicksSurvived * vol;
         } else {
@@ -454,13 +455,16 @@ cave_status tune_class(cave_ctx* ctx, cudaStream_t st, const EngineSim& s, bool 
                 r.SX = p.SX;
                 r.buf[0] = (uint64_t)i * tiled_bytes;
                 r.buf[1] = r.buf[0] + grid_bytes;
-                r.max_ticks = kTrialTicks;
-                r.tick_limit = kTrialTicks;
+                r.max_ticks = T;
+                r.tick_limit = T;
                 r.stop_on_status = 1;
                 r.n_items = (uint32_t)p.items.size();
                 for (int k = 0; k < 3; k++) r.acc_bmin[k] = 0xFFFFFFFFu;
             }
-            if (!ok || items.size() > kMaxItems) continue;
+            if (!ok || items.size() > kMaxItems) {
+                ms = -1;
+                return;
+            }
             for (uint32_t i = 0; i < reps_tiled && e == cudaSuccess; i++)
                 e = cudaMemcpyAsync(reinterpret_cast<unsigned char*>(tpool) + recs[i].buf[0], init, grid_bytes,
                                     cudaMemcpyDeviceToDevice, st);
@@ -469,18 +473,29 @@ cave_status tune_class(cave_ctx* ctx, cudaStream_t st, const EngineSim& s, bool 
             if (e == cudaSuccess)
                 e = cudaMemcpyAsync(titems, items.data(), sizeof(StreamItem) * items.size(), cudaMemcpyHostToDevice, st);
             if (e == cudaSuccess) e = cudaEventRecord(t0, st);
-            for (uint32_t k = 0; k < kTrialTicks && e == cudaSuccess; k++)
+            for (uint32_t k = 0; k < T && e == cudaSuccess; k++)
                 e = launch_stream_tick((int)s.nb, (int)s.nt, nullptr, titems, (uint32_t)items.size(), trecs, tpool, SXp,
                                        SXp, threads, st, k > 0);
             if (e == cudaSuccess) e = cudaEventRecord(t1, st);
             if (e == cudaSuccess)
                 e = cudaMemcpyAsync(recs.data(), trecs, sizeof(StripSim) * reps_tiled, cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-            if (e != cudaSuccess) break;
+            if (e != cudaSuccess) return;
             cudaEventElapsedTime(&ms, t0, t1);
             for (const auto& r : recs) updates += (uint64_t)r.tick * vol;
         }
-        const double rate = ms > 0 ? (double)updates / ms : 0;
+    };
+    double best = -1;
+    ExecChoice best_c = cands[0];
+    for (size_t ci = 0; ci < cands.size() && e == cudaSuccess; ci++) {
+        const ExecChoice& c = cands[ci];
+        uint64_t u1 = 0, u2 = 0;
+        float m1 = 0, m2 = 0;
+        run(c, kTrialTicks, u1, m1);
+        if (e == cudaSuccess && m1 >= 0) run(c, 3 * kTrialTicks, u2, m2);
+        if (e != cudaSuccess) break;
+        if (m1 < 0 || m2 < 0) continue;
+        const double rate = (m2 > m1 && u2 > u1) ? (double)(u2 - u1) / (m2 - m1) : (m2 > 0 ? (double)u2 / m2 : 0);
         if (rate > best) {
             best = rate;
             best_c = c;

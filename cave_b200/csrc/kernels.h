@@ -72,6 +72,21 @@ cudaError_t launch_engine_setup(const EngineJob* jobs, uint32_t n_jobs, uint64_t
                                 const StripSim* recs_in, const uint32_t* rec_slots, uint32_t n_recs, StripSim* recs,
                                 cudaStream_t st);
 
+// ---- render-mode layout (kernels_render.cu)
+struct RenderGeom {
+    uint32_t X, Y, Z, pad;        // cells; ghost shell thickness of the strip grid (wrap: 1)
+    uint32_t Xp, Yp, Zp, SX;      // padded strip grid
+    uint32_t W;                   // texels per row
+    uint64_t elements;            // render buffer elements (8x8x8 texel blocks)
+    uint32_t sdx, sdy, sdz;       // skip grid chunks per axis (8 cells)
+    uint64_t skip_elements;
+};
+RenderGeom render_geometry(uint32_t X, uint32_t Y, uint32_t Z, uint32_t pad);
+cudaError_t launch_render_to_strips(const uint32_t* render, uint4* strips, const RenderGeom& g, cudaStream_t st);
+cudaError_t launch_strips_to_render(const uint4* strips, uint32_t* render, const RenderGeom& g, cudaStream_t st);
+cudaError_t launch_ghost_fill(uint4* strips, const RenderGeom& g, cudaStream_t st);
+cudaError_t launch_render_skip(const uint4* strips, uint32_t* skip, const RenderGeom& g, cudaStream_t st);
+
 // threads = rows * SXp (rows includes the two halo rows), SXp = power of two >= SX, <= 32.
 // nt: sparse term count of the rule (0 = mux tree). param_rule: the rule of every item's
 // simulation when the launch holds one simulation only (passed as a kernel parameter), else null.

@@ -35,7 +35,10 @@
 
 namespace cave {
 
-constexpr int kRing = 4;  // plane slots in flight per CTA
+constexpr int kRing = 8;      // plane slots in flight per CTA (power of two)
+constexpr int kRingLog2 = 3;
+constexpr int kUnroll = 4;    // the grouped march's unroll (divides kRing)
+static_assert((1 << kRingLog2) == kRing && kRing % kUnroll == 0, "ring geometry");
 
 template <int N>
 __device__ __forceinline__ uint4 pack_planes(const uint32_t* p) {
@@ -136,8 +139,10 @@ __global__ void __launch_bounds__(1024) k_stream_tick(const StreamItem* __restri
         mbar_expect_tx(&bars[s], tile_bytes);
         bulk_g2s(slot, g, tile_bytes, &bars[s]);
     };
-    if (threadIdx.x == 0) {
-        for (int f = 0; f < kRing; f++) issue(f, pipe == 2);
+    const uint32_t producer = 0;  // the thread that issues the plane copies
+    const bool grouped = pipe == 2u;
+    if (threadIdx.x == producer) {
+        for (int f = 0; f < kRing; f++) issue(f, grouped);
     }
 
     const uint4* my_ring = ring + (size_t)yy * SX + sx;
@@ -170,35 +175,35 @@ __global__ void __launch_bounds__(1024) k_stream_tick(const StreamItem* __restri
     const size_t xpar = (size_t)rows * SXp;
 
     int zo = zfirst + zstep;
-    if (pipe == 2) {
-        // Grouped order: the plain order below, unrolled by the ring size so that ring slots
-        // and exchange buffers are compile-time constants and the plane rotation needs no
-        // register moves. Every warp waits for the copy of the plane it reads; fetch f is the
+    if (grouped) {
+        // Grouped order: the plain order below, unrolled by kUnroll so that exchange buffers
+        // and slot offsets are fixed within a group and the plane rotation needs no register
+        // moves. Every warp waits for the copy of the plane it reads; fetch f is the
         // (f / kRing)-th use of slot f % kRing, so the phase parity to wait for is (f / kRing) & 1.
         auto read = [&](int f, int s) -> uint4 {  // s == f % kRing
             const int p = zfirst + f * zstep;
             if (f >= nfetch || (unsigned)p >= Z) return make_uint4(0, 0, 0, 0);
-            if (!mbar_wait_bounded(&bars[s], (uint32_t)(f >> 2) & 1u, kWaitLimitNs)) err = kErrWaitTimeout;
+            if (!mbar_wait_bounded(&bars[s], (uint32_t)(f >> kRingLog2) & 1u, kWaitLimitNs)) err = kErrWaitTimeout;
             return has ? my_ring[(size_t)s * slot_stride] : make_uint4(0, 0, 0, 0);
         };
         Row r_m = row_of(read(0, 0));
         uint4 s_c = read(1, 1);
         Row r_c = row_of(s_c);
         __syncthreads();  // slots 0 and 1 consumed
-        if (threadIdx.x == 0) {
+        if (threadIdx.x == producer) {
             fence_proxy_async();
             issue(kRing, true);
             issue(kRing + 1, true);
         }
-        auto body = [&]<int U>(int k) {  // k % kRing == U
-            const uint4 s_in = read(k + 2, (U + 2) & (kRing - 1));
+        auto body = [&]<int U>(int k) {  // k % kUnroll == U
+            const uint4 s_in = read(k + 2, (k + 2) & (kRing - 1));
             const Row r_p = row_of(s_in);
             uint32_t pc[P::NC], ps[P::NS];
             P::make(r_m, r_c, r_p, pc, ps);
             uint4* xb = my_x + (size_t)(U & 1) * xpar;
             *xb = pack_planes<P::NS>(ps);
             __syncthreads();
-            if (threadIdx.x == 0) {
+            if (threadIdx.x == producer) {
                 fence_proxy_async();
                 issue(k + 2 + kRing, true);
             }
@@ -215,8 +220,8 @@ __global__ void __launch_bounds__(1024) k_stream_tick(const StreamItem* __restri
             s_c = s_in;
             zo += zstep;
         };
-        static_assert(kRing == 4, "the grouped march is unrolled by the ring size");
-        for (int k = 0; k < L; k += kRing) {
+        static_assert(kUnroll == 4, "the grouped march is unrolled four times");
+        for (int k = 0; k < L; k += kUnroll) {
             body.template operator()<0>(k);
             if (k + 1 < L) body.template operator()<1>(k + 1);
             if (k + 2 < L) body.template operator()<2>(k + 2);

@@ -348,6 +348,25 @@ cave_status cave_server_fetch(cave_server* s, uint64_t requestId, cave_sim_resul
                               double* latencySeconds);
 cave_status cave_server_get_stats(cave_server* s, cave_server_stats* out);
 
+/* ---- render-mode cell buffers ---------------------------------------------------------- */
+/* Render mode keeps its cells in a different layout (cellStateUtils.slang:18-54, buffer mode):
+ * two cells per texel along x (low nibble = even x), one texel per uint32 element, texels in
+ * 8x8x8 blocks (block-major x, then y, then z) with Morton order inside a block; texel width
+ * ceil(X/2) (simulationRenderer.cpp:58-68). Elements of such a buffer: */
+uint64_t cave_render_buffer_elements(uint32_t X, uint32_t Y, uint32_t Z);
+/* Elements of the skip grid: 8-cell chunks per axis, tiled the same way (simulationRenderer.cpp:86-95). */
+uint64_t cave_render_skip_elements(uint32_t X, uint32_t Y, uint32_t Z);
+/* nticks of the render mode's tick (rayMarchCompute.slang:211-280 computeMain with compute skip
+ * off) on caller-owned DEVICE buffers in that layout: d_in -> d_out (may be the same buffer).
+ * The rule is `params` in bitmask form; the W neighbourhood flag selects wrap-around on every
+ * axis (WRAP_AT_BOUNDARY, simulationRenderer.cpp:595, :623), otherwise out-of-grid cells are
+ * dead. Block-padding elements of d_out are written as 0. d_skip (device, may be NULL)
+ * receives the skip grid the shader scatter-writes for the next frame after the last tick
+ * (:182-205): 1 for every 8-cell chunk within one cell (clamped to the grid, not wrapped) of a
+ * non-zero cell, else 0. X <= 1022. */
+cave_status cave_render_step(cave_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t X, uint32_t Y, uint32_t Z,
+                             const cave_sim_params* params, uint32_t nticks, uint32_t* d_skip);
+
 /* ---- search sweeps (SearchMode + SearchSystem + RuleAggregator) ------------------------ */
 /* The search flags of the reference CLI (src/main.cpp:27-44, startupConfig.h) that shape a
  * sweep. A zero step disables a sweep axis. */

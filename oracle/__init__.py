@@ -114,6 +114,14 @@ def lib():
         L.oracle_run_slot.argtypes = [u32, u32, u32, u64, u64, u64, u64, P(u64), u32, u32, P(u32), u32, i32,
                                       P(SlotResult), sz]
         L.oracle_run_slot.restype = i64
+        L.oracle_render_index.argtypes = [u32, u32, u32, u32, u32, u32]
+        L.oracle_render_index.restype = u64
+        L.oracle_render_elements.argtypes = [u32, u32, u32]
+        L.oracle_render_elements.restype = u64
+        L.oracle_render_skip_elements.argtypes = [u32, u32, u32]
+        L.oracle_render_skip_elements.restype = u64
+        L.oracle_render_step.argtypes = [u32, u32, u32, P(u64), i32, P(u32), P(u32), P(u32)]
+        L.oracle_render_step.restype = None
         _lib = L
     return _lib
 
@@ -269,3 +277,69 @@ def pack(states: np.ndarray) -> np.ndarray:
     for k in range(8):
         out |= full[:, :, :, k] << np.uint32(4 * k)
     return out.reshape(-1)
+
+
+# ---- render-mode layout (cellStateUtils.slang:18-54) -----------------------------------
+def _expand3(v):
+    v = v & 7
+    v = (v | (v << 8)) & 0x100F
+    v = (v | (v << 4)) & 0x10C30C3
+    v = (v | (v << 2)) & 0x1249249
+    return v
+
+
+def render_elements(X, Y, Z) -> int:
+    return int(lib().oracle_render_elements(X, Y, Z))
+
+
+def render_skip_elements(X, Y, Z) -> int:
+    return int(lib().oracle_render_skip_elements(X, Y, Z))
+
+
+def render_indices(X, Y, Z) -> np.ndarray:
+    """Element index of every texel, as an array [Z, Y, ceil(X/2)] (vectorised restatement of
+    cellStateUtils.slang:37-45)."""
+    W = (X + 1) // 2
+    nbx, nby = (W + 7) // 8, (Y + 7) // 8
+    tz, ty, tx = np.meshgrid(np.arange(Z), np.arange(Y), np.arange(W), indexing="ij")
+    block = (tz // 8) * nbx * nby + (ty // 8) * nbx + (tx // 8)
+    m = _expand3(tx % 8) | (_expand3(ty % 8) << 1) | (_expand3(tz % 8) << 2)
+    return (block * 512 + m).astype(np.int64)
+
+
+def render_pack(states: np.ndarray) -> np.ndarray:
+    """uint8 [Z, Y, X] states -> the render mode's tiled buffer (uint32 per texel, 2 cells per
+    texel along x, block padding 0)."""
+    Z, Y, X = states.shape
+    W = (X + 1) // 2
+    full = np.zeros((Z, Y, 2 * W), dtype=np.uint32)
+    full[:, :, :X] = states & 0xF
+    texel = full[:, :, 0::2] | (full[:, :, 1::2] << np.uint32(4))
+    out = np.zeros(render_elements(X, Y, Z), dtype=np.uint32)
+    out[render_indices(X, Y, Z).reshape(-1)] = texel.reshape(-1)
+    return out
+
+
+def render_unpack(buf: np.ndarray, X, Y, Z) -> np.ndarray:
+    W = (X + 1) // 2
+    texel = np.asarray(buf, dtype=np.uint32)[render_indices(X, Y, Z)]
+    full = np.zeros((Z, Y, 2 * W), dtype=np.uint8)
+    full[:, :, 0::2] = texel & 0xF
+    full[:, :, 1::2] = (texel >> 4) & 0xF
+    return full[:, :, :X]
+
+
+def render_step(X, Y, Z, params, buf, wrap, nticks=1, skip=False):
+    """nticks of rayMarchCompute computeMain (compute skip off) on a render-layout buffer.
+    Returns (buffer, skip grid after the last tick or None)."""
+    params = np.ascontiguousarray(params, dtype=np.uint64)
+    cur = np.ascontiguousarray(buf, dtype=np.uint32).copy()
+    sk = None
+    for t in range(nticks):
+        out = np.zeros_like(cur)
+        last = t == nticks - 1
+        sk = np.zeros(render_skip_elements(X, Y, Z), dtype=np.uint32) if (skip and last) else None
+        lib().oracle_render_step(X, Y, Z, _u64p(params), 1 if wrap else 0, _u32p(cur), _u32p(out),
+                                 _u32p(sk) if sk is not None else None)
+        cur = out
+    return cur, sk

@@ -18,9 +18,14 @@
  *   - src/simulation/simulation.h:43-59                        field encodings
  *
  * Parity pin: the reference cannot run here (Vulkan + Slang). The restatement is pinned
- * by (a) hand-derived known-answer tests in tests/test_oracle.py and (b) the historical
- * aggregate viable/possible/unviable counts in benchmarks/reference/debug/
- * bench_results.csv:2-9, reproduced by tests/test_oracle_sweep_counts.py.
+ * by the reference's only exact-value test (cli-rules, src/testing/testRunner.cpp:231-260,
+ * tests/test_rules.py) and by hand-derived known-answer tests (tests/test_oracle.py); the
+ * historical aggregate counts of benchmarks/reference/debug/bench_results.csv:2-9 are a
+ * partial cross-check only (they predate the shader's early-death rule).
+ *
+ * The render-mode step (oracle_render_step) restates shaders/slang/rendering/
+ * rayMarchCompute.slang:60-280 with the packed, Morton-tiled buffer layout of
+ * shaders/slang/common/cellStateUtils.slang:18-54.
  *
  * Two step implementations live here:
  *   oracle_step       -- literal per-cell restatement (up to 26 neighbour reads per cell)
@@ -617,4 +622,127 @@ int64_t oracle_run_slot(uint32_t X, uint32_t Y, uint32_t Z, uint64_t startBirthF
     free(cellsIn);
     free(cellsOut);
     return nres;
+}
+
+
+/* ------------------------------------------------------------------ render-mode layout
+ * cellStateUtils.slang:18-54 (buffer mode): texel (tx, ty, tz) holds cells x = 2tx (low
+ * nibble) and 2tx + 1 (high nibble) in one uint32 element; texels are grouped in 8x8x8
+ * blocks (block-major x, then y, then z), Morton order (x bit 0, y bit 1, z bit 2 of each
+ * triplet) inside a block. Texel width = ceil(X / 2) (simulationRenderer.cpp:58). */
+static uint32_t expand_bits3(uint32_t v) {
+    v &= 7u;
+    v = (v | (v << 8u)) & 0x100Fu;
+    v = (v | (v << 4u)) & 0x10C30C3u;
+    v = (v | (v << 2u)) & 0x1249249u;
+    return v;
+}
+
+uint64_t oracle_render_index(uint32_t tx, uint32_t ty, uint32_t tz, uint32_t X, uint32_t Y, uint32_t Z) {
+    const uint32_t nbx = ((X + 1u) / 2u + 7u) / 8u, nby = (Y + 7u) / 8u;
+    (void)Z;
+    const uint64_t block = (uint64_t)(tz / 8u) * nbx * nby + (uint64_t)(ty / 8u) * nbx + (tx / 8u);
+    const uint32_t m = expand_bits3(tx % 8u) | (expand_bits3(ty % 8u) << 1u) | (expand_bits3(tz % 8u) << 2u);
+    return block * 512u + m;
+}
+
+uint64_t oracle_render_elements(uint32_t X, uint32_t Y, uint32_t Z) {
+    const uint64_t nbx = ((X + 1u) / 2u + 7u) / 8u, nby = (Y + 7u) / 8u, nbz = (Z + 7u) / 8u;
+    return nbx * nby * nbz * 512u;
+}
+
+/* Skip grid of 8-cell chunks, tiled the same way (simulationRenderer.cpp:86-95). */
+uint64_t oracle_render_skip_elements(uint32_t X, uint32_t Y, uint32_t Z) {
+    const uint32_t sx = (X + 7u) / 8u, sy = (Y + 7u) / 8u, sz = (Z + 7u) / 8u;
+    return (uint64_t)((sx + 7u) / 8u) * ((sy + 7u) / 8u) * ((sz + 7u) / 8u) * 512u;
+}
+
+static uint32_t render_cell(const uint32_t *buf, int x, int y, int z, uint32_t X, uint32_t Y, uint32_t Z) {
+    const uint32_t packed = buf[oracle_render_index((uint32_t)x >> 1, (uint32_t)y, (uint32_t)z, X, Y, Z)];
+    return (x & 1) == 0 ? (packed & 0xFu) : ((packed >> 4) & 0xFu);
+}
+
+/* rayMarchCompute.slang:80-113 -- with WRAP_AT_BOUNDARY every axis wraps (no domain
+ * decomposition here), else out-of-grid is not alive. */
+static int render_alive(const uint32_t *buf, int x, int y, int z, uint32_t X, uint32_t Y, uint32_t Z, int wrap,
+                        uint32_t maxCS) {
+    if (wrap) {
+        x = ((x % (int)X) + (int)X) % (int)X;
+        y = ((y % (int)Y) + (int)Y) % (int)Y;
+        z = ((z % (int)Z) + (int)Z) % (int)Z;
+    } else if (x < 0 || x >= (int)X || y < 0 || y >= (int)Y || z < 0 || z >= (int)Z) {
+        return 0;
+    }
+    return render_cell(buf, x, y, z, X, Y, Z) == maxCS;
+}
+
+static uint32_t render_simulate(const uint32_t *buf, int x, int y, int z, uint32_t X, uint32_t Y, uint32_t Z,
+                                int wrap, uint32_t cur, uint32_t maxCS, uint64_t survival, uint64_t birth,
+                                uint32_t flags) {
+    /* rayMarchCompute.slang:121-179 (cube: IsCellViable is always true) */
+    uint32_t n = 0;
+    if (flags & 1u)
+        for (int i = 0; i < 6; i++)
+            n += render_alive(buf, x + kFace[i][0], y + kFace[i][1], z + kFace[i][2], X, Y, Z, wrap, maxCS);
+    if (flags & 2u)
+        for (int i = 0; i < 12; i++)
+            n += render_alive(buf, x + kEdge[i][0], y + kEdge[i][1], z + kEdge[i][2], X, Y, Z, wrap, maxCS);
+    if (flags & 4u)
+        for (int i = 0; i < 8; i++)
+            n += render_alive(buf, x + kCorner[i][0], y + kCorner[i][1], z + kCorner[i][2], X, Y, Z, wrap, maxCS);
+    if (cur == maxCS) return (n > 0u && ((survival >> (n - 1u)) & 1u)) ? maxCS : cur - 1u;
+    if (cur == 0u) return (n > 0u && ((birth >> (n - 1u)) & 1u)) ? maxCS : 0u;
+    return cur - 1u;
+}
+
+/* One tick of rayMarchCompute.slang:211-280 computeMain with compute skip disabled, over
+ * every texel; elements outside the texel grid (block padding) are written as 0. When skip
+ * is given it receives the skip grid the shader scatter-writes for the next frame
+ * (:182-205, chunk size 8, neighbour reach 1 per axis; chunk indices are clamped, not
+ * wrapped), cleared first as computeSystem.cpp:198-250 does. */
+void oracle_render_step(uint32_t X, uint32_t Y, uint32_t Z, const uint64_t params[3], int wrap, const uint32_t *in,
+                        uint32_t *out, uint32_t *skip) {
+    const uint32_t maxCS = (uint32_t)(params[0] >> 60) + 1u;
+    const uint64_t birth = params[0] & PERM_MASK, survival = params[1] & PERM_MASK;
+    const uint32_t flags = (uint32_t)(params[1] >> 60);
+    const uint32_t W = (X + 1u) / 2u;
+    const uint32_t sdx = (X + 7u) / 8u, sdy = (Y + 7u) / 8u, sdz = (Z + 7u) / 8u;
+    memset(out, 0, sizeof(uint32_t) * oracle_render_elements(X, Y, Z));
+    if (skip) memset(skip, 0, sizeof(uint32_t) * oracle_render_skip_elements(X, Y, Z));
+    for (uint32_t tz = 0; tz < Z; tz++)
+        for (uint32_t ty = 0; ty < Y; ty++)
+            for (uint32_t tx = 0; tx < W; tx++) {
+                const uint32_t packed = in[oracle_render_index(tx, ty, tz, X, Y, Z)];
+                const int xa = (int)(2u * tx), xb = xa + 1;
+                const int bvalid = xb < (int)X;
+                const uint32_t na = render_simulate(in, xa, (int)ty, (int)tz, X, Y, Z, wrap, packed & 0xFu, maxCS,
+                                                    survival, birth, flags);
+                const uint32_t nbv = bvalid ? render_simulate(in, xb, (int)ty, (int)tz, X, Y, Z, wrap,
+                                                              (packed >> 4) & 0xFu, maxCS, survival, birth, flags)
+                                            : 0u;
+                out[oracle_render_index(tx, ty, tz, X, Y, Z)] = (nbv << 4) | (na & 0xFu);
+                if (!skip) continue;
+                for (int c = 0; c < 2; c++) {
+                    const int x = c ? xb : xa;
+                    if ((c ? nbv : na) == 0u || (c && !bvalid)) continue;
+                    int lo[3] = {x - 1, (int)ty - 1, (int)tz - 1}, hi[3] = {x + 1, (int)ty + 1, (int)tz + 1};
+                    const int dim[3] = {(int)sdx, (int)sdy, (int)sdz};
+                    for (int a = 0; a < 3; a++) {
+                        lo[a] = lo[a] < 0 ? 0 : lo[a] / 8;  /* floor for lo >= 0; clamp(-1 / 8) to 0 */
+                        hi[a] = hi[a] / 8;
+                        if (hi[a] > dim[a] - 1) hi[a] = dim[a] - 1;
+                    }
+                    for (int k = lo[2]; k <= hi[2]; k++)
+                        for (int j = lo[1]; j <= hi[1]; j++)
+                            for (int i = lo[0]; i <= hi[0]; i++) {
+                                const uint32_t nbx = (sdx + 7u) / 8u, nby = (sdy + 7u) / 8u;
+                                const uint64_t block = (uint64_t)((uint32_t)k / 8u) * nbx * nby +
+                                                       (uint64_t)((uint32_t)j / 8u) * nbx + ((uint32_t)i / 8u);
+                                const uint32_t m = expand_bits3((uint32_t)i % 8u) |
+                                                   (expand_bits3((uint32_t)j % 8u) << 1u) |
+                                                   (expand_bits3((uint32_t)k % 8u) << 2u);
+                                skip[block * 512u + m] = 1u;
+                            }
+                }
+            }
 }
