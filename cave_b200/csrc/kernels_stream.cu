@@ -49,9 +49,11 @@ __device__ __forceinline__ uint4 pack_planes(const uint32_t* p) {
     return v;
 }
 
-// Shared-memory layout (dynamic): ring[kRing][rows*SX] uint4, xch[2][rows*SXp] uint4, mbarriers.
+constexpr int kXch = 2;       // y-exchange buffers (double-buffered)
+
+// Shared-memory layout (dynamic): ring[kRing][rows*SX] uint4, xch[kXch][rows*SXp] uint4, mbarriers.
 __host__ __device__ inline size_t stream_smem_bytes(uint32_t rows, uint32_t SX, uint32_t SXp) {
-    return (size_t)kRing * rows * SX * 16 + (size_t)2 * rows * SXp * 16 + kRing * 8 + 16;
+    return (size_t)kRing * rows * SX * 16 + (size_t)kXch * rows * SXp * 16 + kRing * 8 + 16;
 }
 
 __device__ void fold_tick(StripSim* sim);
@@ -71,7 +73,7 @@ __global__ void __launch_bounds__(1024) k_stream_tick(const StreamItem* __restri
     {
         const uint32_t SXc = sims[it.sim].SX;  // geometry is fixed for the run
         bars = reinterpret_cast<uint64_t*>(reinterpret_cast<uint4*>(smem_raw) + (size_t)kRing * rows * SXc +
-                                           (size_t)2 * rows * SXp);
+                                           (size_t)kXch * rows * SXp);
     }
     if (threadIdx.x == 0) {
         for (int s = 0; s < kRing; s++) mbar_init(&bars[s], 1);
