@@ -32,29 +32,9 @@
 #include "kernels.h"
 #include "ptx.cuh"
 #include "ring.cuh"
+#include "stream_common.cuh"
 
 namespace cave {
-
-constexpr int kRing = 8;      // plane slots in flight per CTA (power of two)
-constexpr int kRingLog2 = 3;
-constexpr int kUnroll = 4;    // the grouped march's unroll (divides kRing)
-static_assert((1 << kRingLog2) == kRing && kRing % kUnroll == 0, "ring geometry");
-
-template <int N>
-__device__ __forceinline__ uint4 pack_planes(const uint32_t* p) {
-    uint4 v = make_uint4(p[0], 0u, 0u, 0u);
-    if constexpr (N > 1) v.y = p[1];
-    if constexpr (N > 2) v.z = p[2];
-    if constexpr (N > 3) v.w = p[3];
-    return v;
-}
-
-constexpr int kXch = 2;       // y-exchange buffers (double-buffered)
-
-// Shared-memory layout (dynamic): ring[kRing][rows*SX] uint4, xch[kXch][rows*SXp] uint4, mbarriers.
-__host__ __device__ inline size_t stream_smem_bytes(uint32_t rows, uint32_t SX, uint32_t SXp) {
-    return (size_t)kRing * rows * SX * 16 + (size_t)kXch * rows * SXp * 16 + kRing * 8 + 16;
-}
 
 __device__ void fold_tick(StripSim* sim);
 
@@ -387,17 +367,10 @@ __global__ void __launch_bounds__(1024) k_stream_tick(const StreamItem* __restri
 __device__ void fold_tick(StripSim* sim) {
     volatile StripSim* vs = sim;
     const uint32_t surv = vs->acc_surv, born = vs->acc_born, zero = vs->acc_zero, pop = vs->acc_pop;
-    const uint32_t volume = sim->X * sim->Y * sim->Z;
-    cave_tick_stats st;
-    st.snapshot.numberOfDeadCells = zero - born;
-    st.snapshot.numberOfCellsBorn = born;
-    st.snapshot.numberOfSurvivingCells = surv;
-    st.snapshot.numberOfDyingCells = volume - (zero - born) - born - surv;
-    st.population = pop;
-    st.changed = born + st.snapshot.numberOfDyingCells;
+    uint32_t bmin[3], bmax[3];
     for (int q = 0; q < 3; q++) {
-        st.bbox_min[q] = vs->acc_bmin[q];
-        st.bbox_max[q] = vs->acc_bmax[q];
+        bmin[q] = vs->acc_bmin[q];
+        bmax[q] = vs->acc_bmax[q];
     }
     sim->acc_surv = sim->acc_born = sim->acc_zero = sim->acc_pop = 0;
     for (int q = 0; q < 3; q++) {
@@ -405,49 +378,8 @@ __device__ void fold_tick(StripSim* sim) {
         sim->acc_bmax[q] = 0;
     }
     sim->ticket = 0;
-    const uint32_t t = sim->tick;
-    if (sim->per_tick) sim->per_tick[t] = st;
-    sim->last = st;
-    sim->total_changed += st.changed;
-    if (st.changed) sim->pop_change_ticks++;
-    // searchManager.slang:115-139
-    cave_grid_info info = sim->info;
-    info.numberOfSimulationTicksSurvived++;
-    info.totalNumberOfCellsThatDied += st.snapshot.numberOfDeadCells;
-    info.totalNumberOfCellsThatWereBorn += born;
-    info.finalAliveCount = surv;
-    if (surv > info.maxAliveCount) info.maxAliveCount = surv;
-    if (surv == 0u && born == 0u)
-        info.status = 1;
-    else if (info.numberOfSimulationTicksSurvived >= sim->max_ticks)
-        info.status = 2;
-    else
-        info.status = 0;
-    sim->info = info;
-    sim->tick = t + 1;
-    const bool done = (sim->stop_on_status && info.status > 0) || t + 1 >= sim->tick_limit;
-    if (done) sim->done = 1;
-    __threadfence();
-    if (done && sim->ring) {
-        cave_sim_result r;
-        r.info = info;
-        r.category = result_category(info, sim->rule.maxcs);
-        r.tag = 0;
-        r.population = st.population;
-        r.activeTicks = sim->pop_change_ticks;
-        r.totalChanged = sim->total_changed;
-        for (int q = 0; q < 3; q++) {
-            r.bbox_min[q] = st.bbox_min[q];
-            r.bbox_max[q] = st.bbox_max[q];
-        }
-        r.params = cave_sim_params{0, 0, 0};
-        r.error = sim->error;
-        r.pad = 0;
-        ring_push(sim->ring, sim->slot, r);
-    }
+    fold_values(sim, surv, born, zero, pop, bmin, bmax);
 }
-
-
 
 // ------------------------------------------------------------------ launch helpers
 // Variant switches for tuning runs: CAVE_STREAM_PIPE (march order: 2 grouped, the default;
