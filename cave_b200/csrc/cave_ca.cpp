@@ -418,9 +418,13 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
     for (int k = 0; k < 3; k++) s.acc_bmin[k] = 0xFFFFFFFFu;
     cave_tick_stats* dticks = nullptr;
     StreamItem* ditems = nullptr;
+    TickTotals* dtt = nullptr;  // per-tick totals: the statistics are folded after the last tick
     if (per_tick && nticks) CAVE_CUDA(ctx, cudaMalloc(&dticks, sizeof(cave_tick_stats) * nticks));
     s.per_tick = dticks;
     cudaError_t e = cudaMalloc(&ditems, sizeof(StreamItem) * plan.items.size());
+    if (e == cudaSuccess && nticks) e = cudaMalloc(&dtt, sizeof(TickTotals) * nticks);
+    if (e == cudaSuccess && nticks) e = cudaMemsetAsync(dtt, 0, sizeof(TickTotals) * nticks, ctx->stream);
+    s.deferred = dtt;
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(ditems, plan.items.data(), sizeof(StreamItem) * plan.items.size(), cudaMemcpyHostToDevice,
                             ctx->stream);
@@ -433,7 +437,8 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
     record(ctx, 2);
     for (uint32_t t = 0; t < nticks && e == cudaSuccess; t++)
         e = launch_stream_tick((int)(d.flags & 7u), (int)s.rule.nterms, &s.rule, ditems, (uint32_t)plan.items.size(),
-                               g->sim, g->strips, plan.SX, plan.SXp, plan.threads, ctx->stream);
+                               g->sim, g->strips, plan.SX, plan.SXp, plan.threads, ctx->stream, true, (int)t);
+    if (e == cudaSuccess && nticks) e = launch_fold_deferred(g->sim, dtt, nticks, ctx->stream);
     record(ctx, 3);
     // Raw stepping never stops early, so the result is in copy (nticks & 1).
     if (e == cudaSuccess)
@@ -450,8 +455,9 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     cudaFree(dticks);
     cudaFree(ditems);
+    cudaFree(dtt);
     if (e != cudaSuccess) return check_cuda(ctx, e, "cave_run");
-    finish_timing(ctx, nticks, nticks + 2, true);
+    finish_timing(ctx, nticks, nticks + 3, true);
     if (back.error & kErrWaitTimeout) return set_error(ctx, CAVE_ERR_TIMEOUT, "streaming kernel: bulk-copy wait timed out");
     if (back.error) return set_error(ctx, CAVE_ERR_INTERNAL, "streaming kernel raised an error flag");
     if (back.tick != nticks) return set_error(ctx, CAVE_ERR_INTERNAL, "streaming run stopped early");

@@ -99,6 +99,16 @@ struct DoneRing {
     DoneEntry* entries;        // device alias of the host-mapped entry array
 };
 
+// One tick's totals of a raw-stepping run whose fold is deferred to the end of the run. The
+// minimum of the bounding box is kept inverted (~min, combined with atomicMax) so that an
+// all-zero slot is the empty state.
+struct TickTotals {
+    uint32_t surv, born, zero, pop;
+    uint32_t nbmin[3], bmax[3];
+    uint32_t pad[2];
+};
+static_assert(sizeof(TickTotals) == 48, "TickTotals layout");
+
 // ---- bit-plane (strip) path -----------------------------------------------------------
 // Per-simulation device record of the strip kernels.
 struct StripSim {
@@ -127,6 +137,8 @@ struct StripSim {
     DoneRing* ring;             // optional: the final result is pushed here when done
     uint32_t slot;              // engine slot reported with the result
     uint32_t pad;
+    TickTotals* deferred;       // raw stepping: per-tick totals, folded after the run (the
+                                // tick launches then take their tick index as an argument)
 };
 
 }  // namespace cave

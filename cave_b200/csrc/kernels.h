@@ -93,8 +93,12 @@ cudaError_t launch_render_skip(const uint4* strips, uint32_t* skip, const Render
 // Launches use programmatic dependent launch, so consecutive ticks overlap set-up and drain.
 // pdl = false launches without the programmatic-dependent-launch attribute (the first tick
 // after a cross-stream event wait).
+// tick_arg >= 0: a deferred-fold run (the one simulation's record has `deferred` set); the
+// launch is tick tick_arg and only adds its totals to deferred[tick_arg].
 cudaError_t launch_stream_tick(int nb, int nt, const DeviceRule* param_rule, const StreamItem* items,
                                uint32_t n_items, StripSim* sims, uint4* pool, uint32_t SX, uint32_t SXp,
-                               uint32_t threads, cudaStream_t st, bool pdl = true);
+                               uint32_t threads, cudaStream_t st, bool pdl = true, int tick_arg = -1);
+// After the last tick of a deferred-fold run: per-tick statistics and the record's GridInfo.
+cudaError_t launch_fold_deferred(StripSim* sim, const TickTotals* tt, uint32_t nticks, cudaStream_t st);
 
 }  // namespace cave

@@ -40,7 +40,7 @@ __device__ void fold_tick(StripSim* sim);
 
 template <int NB, int NT, bool PR>
 __global__ void __launch_bounds__(1024) k_stream_tick(const StreamItem* __restrict__ items, StripSim* sims,
-                                                      uint4* pool, uint32_t sxp_log2, uint32_t pipe,
+                                                      uint4* pool, uint32_t sxp_log2, uint32_t pipe, int tick_arg,
                                                       const __grid_constant__ DeviceRule prule) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ uint32_t s_skip;
@@ -81,7 +81,8 @@ __global__ void __launch_bounds__(1024) k_stream_tick(const StreamItem* __restri
     const DeviceRule& R = PR ? prule : lr;
 
     const uint32_t SX = sim->SX, X = sim->X, Y = sim->Y, Z = sim->Z;
-    const uint32_t tick = sim->tick;
+    // A deferred-fold run (sim->deferred) passes the tick index; otherwise the record counts.
+    const uint32_t tick = tick_arg >= 0 ? (uint32_t)tick_arg : sim->tick;
     const uint4* src = reinterpret_cast<const uint4*>(reinterpret_cast<unsigned char*>(pool) + sim->buf[tick & 1u]);
     uint4* dst = reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(pool) + sim->buf[(tick + 1u) & 1u]);
     uint4* ring = reinterpret_cast<uint4*>(smem_raw);
@@ -342,6 +343,23 @@ __global__ void __launch_bounds__(1024) k_stream_tick(const StreamItem* __restri
             for (int q = 7; q < 10; q++) red[0][q] = max(red[0][q], red[w][q]);
             red[0][10] |= red[w][10];
         }
+        if (tick_arg >= 0) {
+            // deferred fold: add this CTA's totals to the tick's slot (no ticket, no fence:
+            // the next launch starts after this one has completed and flushed)
+            TickTotals* d = sim->deferred + tick;
+            if (red[0][0]) atomicAdd(&d->surv, red[0][0]);
+            if (red[0][1]) atomicAdd(&d->born, red[0][1]);
+            if (red[0][2]) atomicAdd(&d->zero, red[0][2]);
+            if (red[0][3]) {
+                atomicAdd(&d->pop, red[0][3]);
+                for (int q = 0; q < 3; q++) {
+                    atomicMax(&d->nbmin[q], ~red[0][4 + q]);
+                    atomicMax(&d->bmax[q], red[0][7 + q]);
+                }
+            }
+            if (red[0][10]) atomicOr(&sim->error, red[0][10]);
+            return;
+        }
         if (red[0][0]) atomicAdd(&sim->acc_surv, red[0][0]);
         if (red[0][1]) atomicAdd(&sim->acc_born, red[0][1]);
         if (red[0][2]) atomicAdd(&sim->acc_zero, red[0][2]);
@@ -361,6 +379,82 @@ __global__ void __launch_bounds__(1024) k_stream_tick(const StreamItem* __restri
         __threadfence();
         fold_tick(sim);
     }
+}
+
+// The fold of a deferred-fold run, after its last tick: every tick's statistics from its
+// slot, and the record's GridInfo and totals as nticks sequential folds (fold_values) would
+// leave them -- in raw stepping nothing the fold computes feeds back into the stepping.
+// One block; the record must be fresh (tick 0, zero GridInfo and totals).
+__global__ void __launch_bounds__(256) k_fold_deferred(StripSim* sim, const TickTotals* __restrict__ tt,
+                                                       uint32_t nticks) {
+    __shared__ uint32_t s_died[256], s_born[256], s_maxs[256], s_nchg[256];
+    __shared__ unsigned long long s_chg[256];
+    const uint32_t volume = sim->X * sim->Y * sim->Z;
+    cave_tick_stats* per_tick = sim->per_tick;
+    uint32_t died = 0, born_sum = 0, maxs = 0, nchg = 0;
+    unsigned long long chg = 0;
+    for (uint32_t t = threadIdx.x; t < nticks; t += blockDim.x) {
+        const TickTotals v = tt[t];
+        cave_tick_stats st;
+        st.snapshot.numberOfDeadCells = v.zero - v.born;
+        st.snapshot.numberOfCellsBorn = v.born;
+        st.snapshot.numberOfSurvivingCells = v.surv;
+        st.snapshot.numberOfDyingCells = volume - (v.zero - v.born) - v.born - v.surv;
+        st.population = v.pop;
+        st.changed = v.born + st.snapshot.numberOfDyingCells;
+        for (int q = 0; q < 3; q++) {
+            st.bbox_min[q] = ~v.nbmin[q];
+            st.bbox_max[q] = v.bmax[q];
+        }
+        if (per_tick) per_tick[t] = st;
+        if (t + 1 == nticks) sim->last = st;
+        died += st.snapshot.numberOfDeadCells;
+        born_sum += v.born;
+        maxs = max(maxs, v.surv);
+        chg += st.changed;
+        nchg += st.changed ? 1u : 0u;
+    }
+    s_died[threadIdx.x] = died;
+    s_born[threadIdx.x] = born_sum;
+    s_maxs[threadIdx.x] = maxs;
+    s_nchg[threadIdx.x] = nchg;
+    s_chg[threadIdx.x] = chg;
+    __syncthreads();
+    for (uint32_t o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            s_died[threadIdx.x] += s_died[threadIdx.x + o];
+            s_born[threadIdx.x] += s_born[threadIdx.x + o];
+            s_maxs[threadIdx.x] = max(s_maxs[threadIdx.x], s_maxs[threadIdx.x + o]);
+            s_nchg[threadIdx.x] += s_nchg[threadIdx.x + o];
+            s_chg[threadIdx.x] += s_chg[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && nticks) {
+        const TickTotals last = tt[nticks - 1];
+        cave_grid_info info = sim->info;  // searchManager.slang:115-139 over all ticks
+        info.numberOfSimulationTicksSurvived += nticks;
+        info.totalNumberOfCellsThatDied += s_died[0];
+        info.totalNumberOfCellsThatWereBorn += s_born[0];
+        info.finalAliveCount = last.surv;
+        info.maxAliveCount = max(info.maxAliveCount, s_maxs[0]);
+        if (last.surv == 0u && last.born == 0u)
+            info.status = 1;
+        else if (info.numberOfSimulationTicksSurvived >= sim->max_ticks)
+            info.status = 2;
+        else
+            info.status = 0;
+        sim->info = info;
+        sim->total_changed += s_chg[0];
+        sim->pop_change_ticks += s_nchg[0];
+        sim->tick += nticks;
+        if (sim->tick >= sim->tick_limit) sim->done = 1;
+    }
+}
+
+cudaError_t launch_fold_deferred(StripSim* sim, const TickTotals* tt, uint32_t nticks, cudaStream_t st) {
+    k_fold_deferred<<<1, 256, 0, st>>>(sim, tt, nticks);
+    return cudaGetLastError();
 }
 
 // Folds the accumulated statistics of one tick into the simulation record (last CTA).
@@ -400,7 +494,7 @@ static bool stream_pdl() {
 template <int NB, int NT, bool PR>
 static cudaError_t launch_stream_inst(const StreamItem* items, uint32_t n_items, StripSim* sims, uint4* pool,
                                      uint32_t sxp_log2, uint32_t threads, size_t smem, const DeviceRule& rule,
-                                     cudaStream_t st, bool pdl) {
+                                     cudaStream_t st, bool pdl, int tick_arg) {
     auto k = k_stream_tick<NB, NT, PR>;
     static size_t configured = 0;  // largest dynamic shared memory set for this instance
     static std::mutex mu;
@@ -422,26 +516,26 @@ static cudaError_t launch_stream_inst(const StreamItem* items, uint32_t n_items,
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = (pdl && stream_pdl()) ? 1 : 0;
-    return cudaLaunchKernelEx(&cfg, k, items, sims, pool, sxp_log2, stream_pipe(), rule);
+    return cudaLaunchKernelEx(&cfg, k, items, sims, pool, sxp_log2, stream_pipe(), tick_arg, rule);
 }
 
 template <int NB, bool PR>
 static cudaError_t launch_stream_nt(int nt, const StreamItem* items, uint32_t n_items, StripSim* sims, uint4* pool,
                                    uint32_t sxp_log2, uint32_t threads, size_t smem, const DeviceRule& rule,
-                                   cudaStream_t st, bool pdl) {
+                                   cudaStream_t st, bool pdl, int tick_arg) {
     switch (nt) {
-        case 0: return launch_stream_inst<NB, 0, PR>(items, n_items, sims, pool, sxp_log2, threads, smem, rule, st, pdl);
-        case 1: return launch_stream_inst<NB, 1, PR>(items, n_items, sims, pool, sxp_log2, threads, smem, rule, st, pdl);
-        case 2: return launch_stream_inst<NB, 2, PR>(items, n_items, sims, pool, sxp_log2, threads, smem, rule, st, pdl);
-        case 3: return launch_stream_inst<NB, 3, PR>(items, n_items, sims, pool, sxp_log2, threads, smem, rule, st, pdl);
-        case 4: return launch_stream_inst<NB, 4, PR>(items, n_items, sims, pool, sxp_log2, threads, smem, rule, st, pdl);
+        case 0: return launch_stream_inst<NB, 0, PR>(items, n_items, sims, pool, sxp_log2, threads, smem, rule, st, pdl, tick_arg);
+        case 1: return launch_stream_inst<NB, 1, PR>(items, n_items, sims, pool, sxp_log2, threads, smem, rule, st, pdl, tick_arg);
+        case 2: return launch_stream_inst<NB, 2, PR>(items, n_items, sims, pool, sxp_log2, threads, smem, rule, st, pdl, tick_arg);
+        case 3: return launch_stream_inst<NB, 3, PR>(items, n_items, sims, pool, sxp_log2, threads, smem, rule, st, pdl, tick_arg);
+        case 4: return launch_stream_inst<NB, 4, PR>(items, n_items, sims, pool, sxp_log2, threads, smem, rule, st, pdl, tick_arg);
         default: return cudaErrorInvalidValue;
     }
 }
 
 cudaError_t launch_stream_tick(int nb, int nt, const DeviceRule* param_rule, const StreamItem* items,
                                uint32_t n_items, StripSim* sims, uint4* pool, uint32_t SX, uint32_t SXp,
-                               uint32_t threads, cudaStream_t st, bool pdl) {
+                               uint32_t threads, cudaStream_t st, bool pdl, int tick_arg) {
     uint32_t lg = 0;
     while ((1u << lg) < SXp) lg++;
     const uint32_t rows = threads / SXp;
@@ -450,8 +544,8 @@ cudaError_t launch_stream_tick(int nb, int nt, const DeviceRule* param_rule, con
     const DeviceRule& r = param_rule ? *param_rule : dummy;
 #define CAVE_NB_CASE(N)                                                                                        \
     case N:                                                                                                    \
-        return param_rule ? launch_stream_nt<N, true>(nt, items, n_items, sims, pool, lg, threads, smem, r, st, pdl) \
-                          : launch_stream_nt<N, false>(nt, items, n_items, sims, pool, lg, threads, smem, r, st, pdl);
+        return param_rule ? launch_stream_nt<N, true>(nt, items, n_items, sims, pool, lg, threads, smem, r, st, pdl, tick_arg) \
+                          : launch_stream_nt<N, false>(nt, items, n_items, sims, pool, lg, threads, smem, r, st, pdl, tick_arg);
     switch (nb & 7) {
         CAVE_NB_CASE(0)
         CAVE_NB_CASE(1)

@@ -45,17 +45,23 @@ cave_status cave_render_step(cave_ctx* ctx, const uint32_t* d_in, uint32_t* d_ou
     StripSim* rec = nullptr;
     StreamItem* items = nullptr;
     struct Free {
-        void* p[3];
+        void* p[4];
         ~Free() {
             for (void* q : p) cudaFree(q);
         }
-    } fr{{nullptr, nullptr, nullptr}};
+    } fr{{nullptr, nullptr, nullptr, nullptr}};
     CAVE_CUDA(ctx, cudaMalloc(&strips, nstrips * 16 * 2));
     fr.p[0] = strips;
     CAVE_CUDA(ctx, cudaMalloc(&rec, sizeof(StripSim)));
     fr.p[1] = rec;
     CAVE_CUDA(ctx, cudaMalloc(&items, sizeof(StreamItem) * plan.items.size()));
     fr.p[2] = items;
+    TickTotals* tt = nullptr;  // per-tick totals, folded after the last tick
+    if (nticks) {
+        CAVE_CUDA(ctx, cudaMalloc(&tt, sizeof(TickTotals) * nticks));
+        fr.p[3] = tt;
+        CAVE_CUDA(ctx, cudaMemsetAsync(tt, 0, sizeof(TickTotals) * nticks, ctx->stream));
+    }
     StripSim s;
     std::memset(&s, 0, sizeof(s));
     s.rule = make_device_rule(d);
@@ -70,6 +76,7 @@ cave_status cave_render_step(cave_ctx* ctx, const uint32_t* d_in, uint32_t* d_ou
     s.stop_on_status = 0;
     s.n_items = (uint32_t)plan.items.size();
     for (int k = 0; k < 3; k++) s.acc_bmin[k] = 0xFFFFFFFFu;
+    s.deferred = tt;
     cudaError_t e = cudaMemcpyAsync(rec, &s, sizeof(s), cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(items, plan.items.data(), sizeof(StreamItem) * plan.items.size(), cudaMemcpyHostToDevice,
@@ -79,8 +86,9 @@ cave_status cave_render_step(cave_ctx* ctx, const uint32_t* d_in, uint32_t* d_ou
         if (pad) e = launch_ghost_fill(strips + (uint64_t)(t & 1u) * nstrips, g, ctx->stream);
         if (e == cudaSuccess)
             e = launch_stream_tick((int)(d.flags & 7u), (int)s.rule.nterms, &s.rule, items, (uint32_t)plan.items.size(),
-                                   rec, strips, plan.SX, plan.SXp, plan.threads, ctx->stream, t > 0 && !pad);
+                                   rec, strips, plan.SX, plan.SXp, plan.threads, ctx->stream, t > 0 && !pad, (int)t);
     }
+    if (e == cudaSuccess && nticks) e = launch_fold_deferred(rec, tt, nticks, ctx->stream);
     const uint4* last = strips + (uint64_t)(nticks & 1u) * nstrips;
     if (e == cudaSuccess) e = launch_strips_to_render(last, d_out, g, ctx->stream);
     if (e == cudaSuccess && d_skip) e = launch_render_skip(last, d_skip, g, ctx->stream);
