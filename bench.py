@@ -226,11 +226,16 @@ def large_workload(args, world, rank, local, pg):
         flush.zero_()
         torch.cuda.synchronize(local)
 
+    # the tick kernel compiled for this rule (NVRTC, cached), unless CAVE_JIT=off
+    t_prep = time.perf_counter()
+    ctx.prepare_rule(params)
+    prep_s = time.perf_counter() - t_prep
     for _ in range(args.warmup):
         reset()
         g.run(params, T, T, stats=True)
     barrier(pg, local)
     dev_ms, tick_ms, conv_ms, launches = [], [], [], 0
+    _, jit0 = cb.jit_stats()
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             reset()
@@ -242,6 +247,8 @@ def large_workload(args, world, rank, local, pg):
             launches += t.launches
         barrier(pg, local)
     clocks = clk.summary()
+    _, jit1 = cb.jit_stats()
+    specialised = jit1 - jit0 == T * args.steps
     # end-to-end through the C ABI with host buffers
     e2e_ms = []
     for i in range(0 if args.no_e2e else args.steps + 1):
@@ -279,7 +286,10 @@ def large_workload(args, world, rank, local, pg):
                                f"{T} ticks, stats every tick", "grid": [G, G, G], "ticks": T,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "256 MiB buffer written between timed steps (a step is one whole run; within a run each "
-                         "tick reads the previous tick's output)"},
+                         "tick reads the previous tick's output)",
+                   "tick_kernel": ("compiled for the rule at run time (NVRTC, cached; cave_prepare_rule took "
+                                   f"{prep_s:.2f} s before the warm-up)") if specialised else
+                                  "generic (rule read at run time)"},
         "tick_kernel_us": per_launch_s * 1e6,
         "convert_ms_per_step": sum(conv_ms) / len(conv_ms),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

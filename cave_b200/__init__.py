@@ -190,6 +190,9 @@ _SIGS = {
     "cave_grid_seed_threshold": (i32, [ctypes.c_void_p, u32, u32, u32, u64, u32, u32]),
     "cave_step": (i32, [ctypes.c_void_p, P(SimParams), P(u64), u32, u32, u32, P(TickStats)]),
     "cave_run": (i32, [ctypes.c_void_p, P(SimParams), P(u64), u32, u32, u32, u32, P(TickStats), P(GridInfo)]),
+    "cave_prepare_rule": (i32, [ctypes.c_void_p, P(SimParams), P(u64), u32, u32]),
+    "cave_jit_compile": (i32, [P(SimParams), P(u64), u32, u32, ctypes.c_char_p, ctypes.c_size_t]),
+    "cave_jit_stats": (None, [P(u32), P(u64)]),
     "cave_manager_update": (None, [P(GridSnapshot), P(GridInfo), P(SimParams), u64, u64, u32, P(GridInfo),
                                    P(SimParams)]),
     "cave_enumerate_valid_bitmasks": (u64, [u32, u32, P(u64), u64]),
@@ -221,6 +224,22 @@ _SIGS = {
     "cave_rule_string_to_bitmask": (u64, [ctypes.c_char_p]),
     "cave_bitmask_to_rule_string": (u64, [u64, ctypes.c_char_p, u64]),
 }
+
+
+def jit_compile(params: "SimParams", valid=None, max_rule_bits=0):
+    """Compiles the rule-specialised tick kernel without a device. Returns (ok, compiler log)."""
+    v = None if valid is None else np.ascontiguousarray(valid, dtype=np.uint64)
+    buf = ctypes.create_string_buffer(1 << 16)
+    rc = lib().cave_jit_compile(ctypes.byref(params), _u64p(v), 0 if v is None else v.size, max_rule_bits, buf,
+                                len(buf))
+    return rc == 0, buf.value.decode(errors="replace")
+
+
+def jit_stats():
+    """(specialised kernels loaded in this process, tick launches made with them)."""
+    a, b = u32(), u64()
+    lib().cave_jit_stats(ctypes.byref(a), ctypes.byref(b))
+    return a.value, b.value
 
 
 def lib():
@@ -292,6 +311,13 @@ class Context:
 
     def synchronize(self):
         self.check(lib().cave_ctx_synchronize(self.h), "cave_ctx_synchronize")
+
+    def prepare_rule(self, params: SimParams, valid=None, max_rule_bits=0):
+        """Compiles (or loads from the cache) the rule-specialised tick kernel for this rule
+        now, so later streaming runs with it use it (no-op when CAVE_JIT=off)."""
+        v = None if valid is None else np.ascontiguousarray(valid, dtype=np.uint64)
+        self.check(lib().cave_prepare_rule(self.h, ctypes.byref(params), _u64p(v), 0 if v is None else v.size,
+                                           max_rule_bits), "cave_prepare_rule")
 
     def set_timing(self, enable=True):
         self.check(lib().cave_ctx_set_timing(self.h, 1 if enable else 0), "cave_ctx_set_timing")

@@ -29,6 +29,38 @@ def _headers():
         [os.path.join(HERE, "..", "include", "cave_ca.h")]
 
 
+# Device headers NVRTC compiles the rule-specialised tick kernel from (csrc/jit.cpp), by the
+# name each is included under.
+JIT_SOURCES = [(n, os.path.join(CSRC, n)) for n in (
+    "cave_stdint.h", "ca_types.h", "ca_core.cuh", "cave_internal.h", "ptx.cuh", "ring.cuh",
+    "stream_common.cuh", "stream_tick.cuh")] + [("../../include/cave_ca.h", os.path.join(HERE, "..", "include", "cave_ca.h"))]
+_DELIM = "cave_jit_src"
+
+
+def _gen_jit_sources(force=False):
+    """Writes _build/jit_sources.cpp: the JIT headers as string literals (kJitSource*)."""
+    out = os.path.join(OBJ, "jit_sources.cpp")
+    paths = [p for _, p in JIT_SOURCES] + [os.path.abspath(__file__)]
+    if not force and not _stale(out, paths):
+        return out
+    lines = ["// Generated by cave_b200/build.py from the device headers; do not edit.",
+             "namespace cave {",
+             f"extern const int kJitSourceCount = {len(JIT_SOURCES)};",
+             "extern const char* const kJitSourceNames[] = {" + ", ".join(f'"{n}"' for n, _ in JIT_SOURCES) + "};",
+             "extern const char* const kJitSourceTexts[] = {"]
+    for _, p in JIT_SOURCES:
+        text = open(p).read()
+        if f"){_DELIM}\"" in text:
+            raise RuntimeError(f"{p} contains the raw-string delimiter")
+        lines.append(f'R"{_DELIM}({text}){_DELIM}",')
+    lines += ["};", "}  // namespace cave", ""]
+    tmp = out + ".tmp"
+    with open(tmp, "w") as f:
+        f.write("\n".join(lines))
+    os.replace(tmp, out)
+    return out
+
+
 def _stale(target, deps):
     if not os.path.exists(target):
         return True
@@ -53,6 +85,7 @@ def _compile(src, verbose):
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
     srcs = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp")))
+    srcs.append(_gen_jit_sources(force))
     hdrs = _headers()
     todo = [s for s in srcs if force or _stale(os.path.join(OBJ, os.path.basename(s) + ".o"), [s] + hdrs)]
     if todo:

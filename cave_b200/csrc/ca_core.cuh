@@ -22,7 +22,7 @@
 // the cell itself when it is alive; the survival table is shifted one more place for that
 // case (Bn = n + 1 for an alive cell), so no subtraction is needed anywhere.
 #pragma once
-#include <cstdint>
+#include "cave_stdint.h"
 
 #include "ca_types.h"
 

@@ -1,6 +1,6 @@
 // ca_types.h -- rule and geometry types shared by host code and the sm_100a kernels.
 #pragma once
-#include <cstdint>
+#include "cave_stdint.h"
 
 #if defined(__CUDACC__)
 #define CAVE_HD __host__ __device__

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "context.h"
+#include "jit.h"
 #include "kernels.h"
 #include "rules.h"
 
@@ -359,6 +360,37 @@ cave_status cave_run_host(cave_grid* g, const uint32_t* in_words, uint32_t* out_
                     info);
 }
 
+cave_status cave_prepare_rule(cave_ctx* ctx, const cave_sim_params* params, const uint64_t* validBitmasks,
+                              uint32_t nValid, uint32_t maxRuleBits) {
+    if (!ctx || !params) return CAVE_ERR_INVALID_ARG;
+    DecodedRule d;
+    if (!decode_params(*params, validBitmasks, nValid, maxRuleBits, d))
+        return set_error(ctx, CAVE_ERR_INVALID_ARG, "rule index outside the valid-bitmask table");
+    const JitMode jm = jit_mode();
+    if (jm == JitMode::Off) return CAVE_OK;
+    CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
+    const JitKey k = jit_key(make_device_rule(d));
+    if (jit_stream_kernel(k, JitMode::Sync, true)) return CAVE_OK;
+    std::string log;
+    jit_compile(k, &log);
+    return set_error(ctx, CAVE_ERR_INTERNAL, "rule-specialised kernel unavailable: " + log.substr(0, 2000));
+}
+
+cave_status cave_jit_compile(const cave_sim_params* params, const uint64_t* validBitmasks, uint32_t nValid,
+                             uint32_t maxRuleBits, char* log, size_t log_size) {
+    if (!params) return CAVE_ERR_INVALID_ARG;
+    DecodedRule d;
+    if (!decode_params(*params, validBitmasks, nValid, maxRuleBits, d)) return CAVE_ERR_INVALID_ARG;
+    std::string text;
+    const bool ok = jit_compile(jit_key(make_device_rule(d)), &text);
+    if (log && log_size) {
+        const size_t n = std::min(text.size(), log_size - 1);
+        std::memcpy(log, text.data(), n);
+        log[n] = '\0';
+    }
+    return ok ? CAVE_OK : CAVE_ERR_INTERNAL;
+}
+
 cave_status cave_ctx_set_timing(cave_ctx* ctx, int enable) {
     if (!ctx) return CAVE_ERR_INVALID_ARG;
     CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -435,9 +467,16 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
     record(ctx, 1);
     if (e == cudaSuccess) e = launch_nib_to_strips(g->nib[g->cur], g->strips, g->X, g->Y, g->Z, ctx->stream);
     record(ctx, 2);
+    // the rule-specialised kernel when one is ready (jit.h), else the generic one
+    const JitMode jm = jit_mode();
+    const cudaKernel_t jk =
+        nticks ? jit_stream_kernel(jit_key(s.rule), jm, (uint64_t)g->X * g->Y * g->Z >= kJitMinCells) : nullptr;
     for (uint32_t t = 0; t < nticks && e == cudaSuccess; t++)
-        e = launch_stream_tick((int)(d.flags & 7u), (int)s.rule.nterms, &s.rule, ditems, (uint32_t)plan.items.size(),
-                               g->sim, g->strips, plan.SX, plan.SXp, plan.threads, ctx->stream, true, (int)t);
+        e = jk ? launch_stream_tick_jit(jk, ditems, (uint32_t)plan.items.size(), g->sim, g->strips, plan.SX,
+                                        plan.SXp, plan.threads, ctx->stream, true, (int)t)
+               : launch_stream_tick((int)(d.flags & 7u), (int)s.rule.nterms, &s.rule, ditems,
+                                    (uint32_t)plan.items.size(), g->sim, g->strips, plan.SX, plan.SXp, plan.threads,
+                                    ctx->stream, true, (int)t);
     if (e == cudaSuccess && nticks) e = launch_fold_deferred(g->sim, dtt, nticks, ctx->stream);
     record(ctx, 3);
     // Raw stepping never stops early, so the result is in copy (nticks & 1).

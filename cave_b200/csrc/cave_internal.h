@@ -1,10 +1,12 @@
 // cave_internal.h -- device-side records shared by the kernels and the host library.
 #pragma once
-#include <cstdint>
+#include "cave_stdint.h"
 
 #include "../../include/cave_ca.h"
 #include "ca_types.h"
+#ifndef __CUDACC_RTC__
 #include <vector_types.h>
+#endif
 
 namespace cave {
 
@@ -110,6 +112,15 @@ struct TickTotals {
 static_assert(sizeof(TickTotals) == 48, "TickTotals layout");
 
 // ---- bit-plane (strip) path -----------------------------------------------------------
+// One CTA's share of one tick of one simulation in the streaming kernel.
+struct StreamItem {
+    uint32_t sim;            // index into the StripSim array
+    uint16_t y0, ty;         // output rows [y0, y0 + ty)
+    uint16_t z0, z1;         // output planes [z0, z1)
+    uint32_t dir_items;      // bit 0: march towards +z (0) or -z (1); bits 1..31: the number of
+                             // work items of `sim` in this launch (the last one to finish folds)
+};
+
 // Per-simulation device record of the strip kernels.
 struct StripSim {
     DeviceRule rule;

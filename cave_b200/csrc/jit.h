@@ -1,0 +1,56 @@
+// jit.h -- rule-specialised streaming tick kernels, compiled at run time with NVRTC.
+//
+// The library's own tick kernel reads the rule (state count, survival and birth tables) at run
+// time, which costs logic operations on every strip: the alive test compares four planes with
+// the maxCellState bits, and the tables are matched term by term. Compiled with the rule as
+// compile-time constants (stream_tick.cuh with a Fixed rule), the same source folds those into
+// the fewest operations for that rule. Kernels are keyed by (neighbourhood, maxCellState,
+// survival table, birth table), kept per process and, as cubins, in an on-disk cache.
+//
+// Modes (environment variable CAVE_JIT): "off"/"0" never specialise; "async" (the default)
+// starts a background compile the first time a large grid meets a rule and keeps using the
+// generic kernel until the specialised one is ready; "sync"/"1" compiles before the first
+// launch for every grid size. cave_prepare_rule() compiles ahead of time in any mode but off.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "cave_internal.h"
+
+namespace cave {
+
+enum class JitMode { Off, Async, Sync };
+JitMode jit_mode();
+
+struct JitKey {
+    uint32_t nb;      // neighbourhood bits (F=1 E=2 C=4)
+    uint32_t maxcs;   // 1..16
+    uint32_t lut_s;   // DeviceRule::lut_s / lut_b (count-indexed tables)
+    uint32_t lut_b;
+};
+inline JitKey jit_key(const DeviceRule& r) { return JitKey{r.flags & 7u, r.maxcs, r.lut_s, r.lut_b}; }
+
+// Grids at least this large (cells) start a background compile in async mode.
+constexpr uint64_t kJitMinCells = 1ull << 21;
+
+// The specialised kernel for `k` if it is ready (loaded into the runtime), else nullptr. In
+// sync mode a missing kernel is compiled first; in async mode a compile is queued when `start`
+// is set. A key whose compile failed stays on the generic kernel.
+cudaKernel_t jit_stream_kernel(const JitKey& k, JitMode mode, bool start);
+
+// Compiles the kernel for `k` into the caches (no device needed). Returns false with the
+// compiler's log (or the reason NVRTC is unavailable) in *log.
+bool jit_compile(const JitKey& k, std::string* log);
+
+// Launches one tick with a specialised kernel: the arguments of launch_stream_tick without the
+// rule (it is compiled in) and the march order (always grouped).
+cudaError_t launch_stream_tick_jit(cudaKernel_t k, const StreamItem* items, uint32_t n_items, StripSim* sims,
+                                   uint4* pool, uint32_t SX, uint32_t SXp, uint32_t threads, cudaStream_t st,
+                                   bool pdl, int tick_arg);
+
+// Process-wide counters behind cave_jit_stats.
+void jit_count_launch();
+void jit_counts(uint32_t* loaded, uint64_t* launches);
+
+}  // namespace cave

@@ -18,15 +18,6 @@ struct SeedSpec {
     uint32_t maxcs;          // written as (maxcs & 0xF)
 };
 
-// One CTA's share of one tick of one simulation in the streaming kernel.
-struct StreamItem {
-    uint32_t sim;            // index into the StripSim array
-    uint16_t y0, ty;         // output rows [y0, y0 + ty)
-    uint16_t z0, z1;         // output planes [z0, z1)
-    uint32_t dir_items;      // bit 0: march towards +z (0) or -z (1); bits 1..31: the number of
-                             // work items of `sim` in this launch (the last one to finish folds)
-};
-
 cudaError_t launch_plain_step(const uint32_t* in, uint32_t* out, uint32_t X, uint32_t Y, uint32_t Z,
                               PlainSlot* slot, const uint64_t* valid, uint32_t nValid, uint32_t maxRuleBits,
                               cudaStream_t stream);

@@ -1,7 +1,7 @@
 // ptx.cuh -- inline-PTX helpers for mbarriers and TMA bulk copies (sm_90+ forms used on sm_100a).
 // Only non-multicast bulk copies are used anywhere in this library.
 #pragma once
-#include <cstdint>
+#include "cave_stdint.h"
 
 namespace cave {
 

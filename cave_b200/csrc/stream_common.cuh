@@ -1,7 +1,7 @@
 // stream_common.cuh -- ring geometry, shared-memory layout and the per-tick fold of the
 // streaming tick kernel (kernels_stream.cu).
 #pragma once
-#include <cstdint>
+#include "cave_stdint.h"
 
 #include "cave_internal.h"
 #include "ring.cuh"
@@ -87,6 +87,24 @@ __device__ __forceinline__ void fold_values(StripSim* sim, uint32_t surv, uint32
         r.pad = 0;
         ring_push(sim->ring, sim->slot, r);
     }
+}
+
+// Folds the accumulated statistics of one tick into the simulation record (last CTA).
+__device__ inline void fold_tick(StripSim* sim) {
+    volatile StripSim* vs = sim;
+    const uint32_t surv = vs->acc_surv, born = vs->acc_born, zero = vs->acc_zero, pop = vs->acc_pop;
+    uint32_t bmin[3], bmax[3];
+    for (int q = 0; q < 3; q++) {
+        bmin[q] = vs->acc_bmin[q];
+        bmax[q] = vs->acc_bmax[q];
+    }
+    sim->acc_surv = sim->acc_born = sim->acc_zero = sim->acc_pop = 0;
+    for (int q = 0; q < 3; q++) {
+        sim->acc_bmin[q] = 0xFFFFFFFFu;
+        sim->acc_bmax[q] = 0;
+    }
+    sim->ticket = 0;
+    fold_values(sim, surv, born, zero, pop, bmin, bmax);
 }
 
 }  // namespace cave

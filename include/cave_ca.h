@@ -18,8 +18,10 @@
 #ifndef CAVE_CA_H
 #define CAVE_CA_H
 
+#ifndef __CUDACC_RTC__ /* NVRTC has no C library headers; the kernel sources declare the types */
 #include <stddef.h>
 #include <stdint.h>
+#endif
 
 #ifdef __cplusplus
 extern "C" {
@@ -173,6 +175,34 @@ cave_status cave_run_host(cave_grid* g, const uint32_t* in_words, uint32_t* out_
                           const cave_sim_params* params, const uint64_t* validBitmasks, uint32_t nValid,
                           uint32_t maxRuleBits, uint32_t nticks, uint32_t maxTicks, cave_tick_stats* per_tick,
                           cave_grid_info* info);
+
+/* ---- rule-specialised tick kernels ----------------------------------------------------
+ * The reference builds one compute pipeline per shader, with the rule read from a buffer on
+ * every cell (searchSystem.cpp:419, computePipeline.cpp:11-29). Here cave_run and
+ * cave_render_step may run a tick kernel compiled for the rule itself (NVRTC, sm_100a): the
+ * rule's state count and tables become compile-time constants, which removes per-cell logic.
+ * Results are identical either way. Environment variable CAVE_JIT selects the policy: "async"
+ * (default; the first run of a grid of at least 2^21 cells with a new rule starts a
+ * background compile and the following runs use the specialised kernel once it is ready),
+ * "sync" (compile before the first launch, any grid size) or "off". Compiled kernels are
+ * cached per process and on disk (CAVE_JIT_CACHE, default ~/.cache/cave_b200; "off" disables
+ * it).
+ *
+ * cave_prepare_rule: compiles (or loads from the cache) the specialised kernel for this rule
+ * and neighbourhood now, so that every later cave_run / cave_render_step with it uses it.
+ * Returns CAVE_OK (a no-op when CAVE_JIT=off), CAVE_ERR_INVALID_ARG for a rule index outside
+ * the table, or CAVE_ERR_INTERNAL when the kernel could not be compiled or loaded (reason in
+ * cave_last_error; runs then use the generic kernel). */
+cave_status cave_prepare_rule(cave_ctx* ctx, const cave_sim_params* params, const uint64_t* validBitmasks,
+                              uint32_t nValid, uint32_t maxRuleBits);
+/* Compiles the specialised kernel for a rule without any device (fills the caches; e.g. on a
+ * build host with the same disk cache). log (may be NULL) receives up to log_size-1 bytes of
+ * the compiler's output. Returns CAVE_OK, CAVE_ERR_INVALID_ARG or CAVE_ERR_INTERNAL. */
+cave_status cave_jit_compile(const cave_sim_params* params, const uint64_t* validBitmasks, uint32_t nValid,
+                             uint32_t maxRuleBits, char* log, size_t log_size);
+/* Diagnostics: rule-specialised kernels loaded into this process so far, and tick launches
+ * made with them. Either pointer may be NULL. */
+void cave_jit_stats(uint32_t* loaded, uint64_t* launches);
 
 /* cave_run without any device allocation. No counterpart in the reference (its buffers are
  * always created per slot, searchSystem.cpp:126-394); it exists for callers that must not
