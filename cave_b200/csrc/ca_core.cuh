@@ -210,20 +210,32 @@ __device__ __forceinline__ void combine(const uint32_t* pc, const uint32_t* psm,
 }
 
 // ---------------------------------------------------------------- state update + stats
+// acc + v as an integer multiply-add by `one`, so that the add issues on the FMA pipe instead of
+// the integer ALU, which the cell logic keeps busy. `one` must be 1 at run time in a way the
+// compiler cannot see (it would fold the product back into an add on the ALU).
+__device__ __forceinline__ uint32_t mad_add(uint32_t acc, uint32_t v, uint32_t one) {
+    uint32_t r;
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(v), "r"(one), "r"(acc));
+    return r;
+}
+
 struct TickAcc {  // per-thread accumulators for one tick
     uint32_t surviving, born, zero, population;
     uint32_t zmin, zmax;  // z-extent of the thread's non-zero strips
-    __device__ void reset() {
+    uint32_t one;         // 1, opaque to the compiler (see mad_add)
+    __device__ void reset(uint32_t opaque_one = 1u) {
         surviving = born = zero = population = 0u;
         zmin = 0xFFFFFFFFu;
         zmax = 0u;
+        one = opaque_one;
     }
 };
 
 // New state of one strip. s: current state planes; a: its alive plane; valid: cells < X;
 // xbits accumulates the OR of the strip's non-zero masks (its x-extent). The statistics are
-// accumulated only when `count` is set (strips this thread owns, not halo copies).
-template <int NB, int NT>
+// accumulated only when `count` is set (strips this thread owns, not halo copies); cells that
+// were 0 only with kCountZero (a caller may derive them from the previous tick's population).
+template <int NB, int NT, bool kCountZero = true>
 __device__ __forceinline__ uint4 update_strip(uint4 s, uint32_t a, const uint32_t* cnt, uint32_t valid,
                                               const DeviceRule& r, TickAcc& acc, uint32_t& xbits, uint32_t z,
                                               bool count = true) {
@@ -248,11 +260,11 @@ __device__ __forceinline__ uint4 update_strip(uint4 s, uint32_t a, const uint32_
     n.z = (set & r.m[2]) | (~set & d2);
     n.w = (set & r.m[3]) | (~set & d3);
     if (count) {
-        acc.surviving += __popc(sv);
-        acc.born += __popc(bn);
-        acc.zero += __popc(zero);
+        acc.surviving = mad_add(acc.surviving, __popc(sv), acc.one);
+        acc.born = mad_add(acc.born, __popc(bn), acc.one);
+        if constexpr (kCountZero) acc.zero = mad_add(acc.zero, __popc(zero), acc.one);
         const uint32_t nn = n.x | n.y | n.z | n.w;
-        acc.population += __popc(nn);
+        acc.population = mad_add(acc.population, __popc(nn), acc.one);
         xbits |= nn;
         const bool any = nn != 0u;
         acc.zmin = any ? min(acc.zmin, z) : acc.zmin;

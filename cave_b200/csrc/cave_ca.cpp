@@ -469,15 +469,16 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
     record(ctx, 2);
     // the rule-specialised kernel when one is ready (jit.h), else the generic one
     const JitMode jm = jit_mode();
-    const cudaKernel_t jk =
-        nticks ? jit_stream_kernel(jit_key(s.rule), jm, (uint64_t)g->X * g->Y * g->Z >= kJitMinCells) : nullptr;
+    // (its first tick counts every statistic; later ticks leave the zero cells to the fold)
+    const JitKernels jk = nticks ? jit_stream_kernel(jit_key(s.rule), jm, (uint64_t)g->X * g->Y * g->Z >= kJitMinCells)
+                                 : JitKernels{};
     for (uint32_t t = 0; t < nticks && e == cudaSuccess; t++)
-        e = jk ? launch_stream_tick_jit(jk, ditems, (uint32_t)plan.items.size(), g->sim, g->strips, plan.SX,
-                                        plan.SXp, plan.threads, ctx->stream, true, (int)t)
+        e = jk ? launch_stream_tick_jit(t ? jk.derived : jk.counting, ditems, (uint32_t)plan.items.size(), g->sim,
+                                        g->strips, plan.SX, plan.SXp, plan.threads, ctx->stream, true, (int)t)
                : launch_stream_tick((int)(d.flags & 7u), (int)s.rule.nterms, &s.rule, ditems,
                                     (uint32_t)plan.items.size(), g->sim, g->strips, plan.SX, plan.SXp, plan.threads,
                                     ctx->stream, true, (int)t);
-    if (e == cudaSuccess && nticks) e = launch_fold_deferred(g->sim, dtt, nticks, ctx->stream);
+    if (e == cudaSuccess && nticks) e = launch_fold_deferred(g->sim, dtt, nticks, (bool)jk, ctx->stream);
     record(ctx, 3);
     // Raw stepping never stops early, so the result is in copy (nticks & 1).
     if (e == cudaSuccess)

@@ -110,6 +110,11 @@ struct TickTotals {
     uint32_t pad[2];
 };
 static_assert(sizeof(TickTotals) == 48, "TickTotals layout");
+// The tick kernel adds its four sums to surv + 0..3 (and acc_surv + 0..3 of StripSim).
+// (Checked by nvcc and the host compiler; NVRTC has no offsetof.)
+#ifndef __CUDACC_RTC__
+static_assert(__builtin_offsetof(TickTotals, pop) == __builtin_offsetof(TickTotals, surv) + 12, "TickTotals sums");
+#endif
 
 // ---- bit-plane (strip) path -----------------------------------------------------------
 // One CTA's share of one tick of one simulation in the streaming kernel.
@@ -151,5 +156,8 @@ struct StripSim {
     TickTotals* deferred;       // raw stepping: per-tick totals, folded after the run (the
                                 // tick launches then take their tick index as an argument)
 };
+#ifndef __CUDACC_RTC__
+static_assert(__builtin_offsetof(StripSim, acc_pop) == __builtin_offsetof(StripSim, acc_surv) + 12, "StripSim sums");
+#endif
 
 }  // namespace cave

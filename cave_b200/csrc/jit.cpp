@@ -58,11 +58,18 @@ struct JitRule {
 extern "C" __global__ void __launch_bounds__(1024)
 cave_stream_tick_jit(const cave::StreamItem* __restrict__ items, cave::StripSim* sims, uint4* pool,
                      uint32_t sxp_log2, int tick_arg) {
-    cave::stream_tick_body<CAVE_JIT_NB, 0, false, cave::JitRule>(items, sims, pool, sxp_log2, 2u, tick_arg,
-                                                                cave::DeviceRule{});
+    cave::stream_tick_body<CAVE_JIT_NB, 0, false, cave::JitRule, true>(items, sims, pool, sxp_log2, tick_arg,
+                                                                      cave::DeviceRule{});
+}
+extern "C" __global__ void __launch_bounds__(1024)
+cave_stream_tick_jit_derived(const cave::StreamItem* __restrict__ items, cave::StripSim* sims, uint4* pool,
+                             uint32_t sxp_log2, int tick_arg) {
+    cave::stream_tick_body<CAVE_JIT_NB, 0, false, cave::JitRule, false>(items, sims, pool, sxp_log2, tick_arg,
+                                                                       cave::DeviceRule{});
 }
 )cave_unit";
 const char* const kJitKernelName = "cave_stream_tick_jit";
+const char* const kJitDerivedName = "cave_stream_tick_jit_derived";
 
 struct Nvrtc {
     bool ok = false;
@@ -236,7 +243,7 @@ struct Entry {
     std::vector<char> cubin;
     std::string log;
     cudaLibrary_t lib = nullptr;
-    cudaKernel_t kern = nullptr;
+    JitKernels kern;
 };
 using Key = std::tuple<uint32_t, uint32_t, uint32_t, uint32_t>;
 Key key_of(const JitKey& k) { return Key{k.nb, k.maxcs, k.lut_s, k.lut_b}; }
@@ -317,32 +324,34 @@ JitMode jit_mode() {
     return JitMode::Async;
 }
 
-cudaKernel_t jit_stream_kernel(const JitKey& k, JitMode mode, bool start) {
-    if (mode == JitMode::Off) return nullptr;
+JitKernels jit_stream_kernel(const JitKey& k, JitMode mode, bool start) {
+    if (mode == JitMode::Off) return JitKernels{};
     Registry& R = registry();
     std::unique_lock<std::mutex> lk(R.mu);
     Entry* e = &R.entries[key_of(k)];
     if (e->state == State::Loaded) return e->kern;
-    if (e->state == State::Failed) return nullptr;
+    if (e->state == State::Failed) return JitKernels{};
     if (mode == JitMode::Sync) {
         R.compile_now(lk, k);
         e = &R.entries[key_of(k)];
     } else if (e->state == State::None) {
-        if (!start) return nullptr;
+        if (!start) return JitKernels{};
         e->state = State::Queued;
         R.queue.push_back(k);
         if (!R.worker.joinable()) R.worker = std::thread([&R] { R.run(); });
         R.cv.notify_all();
-        return nullptr;
+        return JitKernels{};
     }
-    if (e->state != State::Compiled) return nullptr;
+    if (e->state != State::Compiled) return JitKernels{};
     cudaError_t err = cudaLibraryLoadData(&e->lib, e->cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
-    if (err == cudaSuccess) err = cudaLibraryGetKernel(&e->kern, e->lib, kJitKernelName);
+    if (err == cudaSuccess) err = cudaLibraryGetKernel(&e->kern.counting, e->lib, kJitKernelName);
+    if (err == cudaSuccess) err = cudaLibraryGetKernel(&e->kern.derived, e->lib, kJitDerivedName);
     if (err != cudaSuccess) {
         (void)cudaGetLastError();
         e->state = State::Failed;
+        e->kern = JitKernels{};
         e->log = std::string("loading the specialised kernel: ") + cudaGetErrorString(err);
-        return nullptr;
+        return JitKernels{};
     }
     e->cubin.clear();
     e->cubin.shrink_to_fit();

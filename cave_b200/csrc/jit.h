@@ -34,10 +34,19 @@ inline JitKey jit_key(const DeviceRule& r) { return JitKey{r.flags & 7u, r.maxcs
 // Grids at least this large (cells) start a background compile in async mode.
 constexpr uint64_t kJitMinCells = 1ull << 21;
 
-// The specialised kernel for `k` if it is ready (loaded into the runtime), else nullptr. In
-// sync mode a missing kernel is compiled first; in async mode a compile is queued when `start`
+// The two specialised kernels of one key: `counting` counts every statistic; `derived` leaves
+// out the cells that were 0 before the tick, which a deferred fold derives from the previous
+// tick's population (every tick of a run after its first).
+struct JitKernels {
+    cudaKernel_t counting = nullptr;
+    cudaKernel_t derived = nullptr;
+    explicit operator bool() const { return counting != nullptr; }
+};
+
+// The specialised kernels for `k` if they are ready (loaded into the runtime), else empty. In
+// sync mode a missing key is compiled first; in async mode a compile is queued when `start`
 // is set. A key whose compile failed stays on the generic kernel.
-cudaKernel_t jit_stream_kernel(const JitKey& k, JitMode mode, bool start);
+JitKernels jit_stream_kernel(const JitKey& k, JitMode mode, bool start);
 
 // Compiles the kernel for `k` into the caches (no device needed). Returns false with the
 // compiler's log (or the reason NVRTC is unavailable) in *log.

@@ -90,6 +90,8 @@ cudaError_t launch_stream_tick(int nb, int nt, const DeviceRule* param_rule, con
                                uint32_t n_items, StripSim* sims, uint4* pool, uint32_t SX, uint32_t SXp,
                                uint32_t threads, cudaStream_t st, bool pdl = true, int tick_arg = -1);
 // After the last tick of a deferred-fold run: per-tick statistics and the record's GridInfo.
-cudaError_t launch_fold_deferred(StripSim* sim, const TickTotals* tt, uint32_t nticks, cudaStream_t st);
+// derive_zero: ticks after the first did not count their zero cells (volume - previous population).
+cudaError_t launch_fold_deferred(StripSim* sim, const TickTotals* tt, uint32_t nticks, bool derive_zero,
+                                 cudaStream_t st);
 
 }  // namespace cave

@@ -17,9 +17,9 @@ namespace cave {
 
 template <int NB, int NT, bool PR>
 __global__ void __launch_bounds__(1024) k_stream_tick(const StreamItem* __restrict__ items, StripSim* sims,
-                                                      uint4* pool, uint32_t sxp_log2, uint32_t pipe, int tick_arg,
+                                                      uint4* pool, uint32_t sxp_log2, int tick_arg,
                                                       const __grid_constant__ DeviceRule prule) {
-    stream_tick_body<NB, NT, PR, RuntimeRule>(items, sims, pool, sxp_log2, pipe, tick_arg, prule);
+    stream_tick_body<NB, NT, PR, RuntimeRule>(items, sims, pool, sxp_log2, tick_arg, prule);
 }
 
 // The fold of a deferred-fold run, after its last tick: every tick's statistics from its
@@ -27,7 +27,7 @@ __global__ void __launch_bounds__(1024) k_stream_tick(const StreamItem* __restri
 // leave them -- in raw stepping nothing the fold computes feeds back into the stepping.
 // One block; the record must be fresh (tick 0, zero GridInfo and totals).
 __global__ void __launch_bounds__(256) k_fold_deferred(StripSim* sim, const TickTotals* __restrict__ tt,
-                                                       uint32_t nticks) {
+                                                       uint32_t nticks, uint32_t derive_zero) {
     __shared__ uint32_t s_died[256], s_born[256], s_maxs[256], s_nchg[256];
     __shared__ unsigned long long s_chg[256];
     const uint32_t volume = sim->X * sim->Y * sim->Z;
@@ -35,7 +35,10 @@ __global__ void __launch_bounds__(256) k_fold_deferred(StripSim* sim, const Tick
     uint32_t died = 0, born_sum = 0, maxs = 0, nchg = 0;
     unsigned long long chg = 0;
     for (uint32_t t = threadIdx.x; t < nticks; t += blockDim.x) {
-        const TickTotals v = tt[t];
+        TickTotals v = tt[t];
+        // a tick that did not count its zero cells: they are the cells that were 0 after the
+        // previous tick (every cell outside the population)
+        if (derive_zero && t > 0) v.zero = volume - tt[t - 1].pop;
         cave_tick_stats st;
         st.snapshot.numberOfDeadCells = v.zero - v.born;
         st.snapshot.numberOfCellsBorn = v.born;
@@ -93,22 +96,17 @@ __global__ void __launch_bounds__(256) k_fold_deferred(StripSim* sim, const Tick
     }
 }
 
-cudaError_t launch_fold_deferred(StripSim* sim, const TickTotals* tt, uint32_t nticks, cudaStream_t st) {
-    k_fold_deferred<<<1, 256, 0, st>>>(sim, tt, nticks);
+cudaError_t launch_fold_deferred(StripSim* sim, const TickTotals* tt, uint32_t nticks, bool derive_zero,
+                                 cudaStream_t st) {
+    k_fold_deferred<<<1, 256, 0, st>>>(sim, tt, nticks, derive_zero ? 1u : 0u);
     return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------ launch helpers
-// Variant switches for tuning runs: CAVE_STREAM_PIPE (march order: 2 grouped, the default;
-// 0 plain; 1 software-pipelined) and CAVE_STREAM_PDL (programmatic dependent launch between
-// ticks, default 1).
+// CAVE_STREAM_PDL=0 launches the ticks without programmatic dependent launch (tuning runs).
 static uint32_t env_flag(const char* name, uint32_t dflt) {
     const char* v = std::getenv(name);
     return v ? (uint32_t)std::atoi(v) : dflt;
-}
-static uint32_t stream_pipe() {
-    static const uint32_t v = env_flag("CAVE_STREAM_PIPE", 2);
-    return v;
 }
 static bool stream_pdl() {
     static const bool v = env_flag("CAVE_STREAM_PDL", 1) != 0;
@@ -139,7 +137,7 @@ static cudaError_t launch_stream_inst(const StreamItem* items, uint32_t n_items,
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = (pdl && stream_pdl()) ? 1 : 0;
-    return cudaLaunchKernelEx(&cfg, k, items, sims, pool, sxp_log2, stream_pipe(), tick_arg, rule);
+    return cudaLaunchKernelEx(&cfg, k, items, sims, pool, sxp_log2, tick_arg, rule);
 }
 
 template <int NB, bool PR>

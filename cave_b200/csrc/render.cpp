@@ -84,19 +84,20 @@ cave_status cave_render_step(cave_ctx* ctx, const uint32_t* d_in, uint32_t* d_ou
                             ctx->stream);
     if (e == cudaSuccess) e = launch_render_to_strips(d_in, strips, g, ctx->stream);
     // the rule-specialised kernel when one is ready (jit.h), else the generic one
-    const cudaKernel_t jk =
-        nticks ? jit_stream_kernel(jit_key(s.rule), jit_mode(), (uint64_t)X * Y * Z >= kJitMinCells) : nullptr;
+    // (its first tick counts every statistic; later ticks leave the zero cells to the fold)
+    const JitKernels jk =
+        nticks ? jit_stream_kernel(jit_key(s.rule), jit_mode(), (uint64_t)X * Y * Z >= kJitMinCells) : JitKernels{};
     for (uint32_t t = 0; t < nticks && e == cudaSuccess; t++) {
         if (pad) e = launch_ghost_fill(strips + (uint64_t)(t & 1u) * nstrips, g, ctx->stream);
         const bool pdl = t > 0 && !pad;
         if (e == cudaSuccess)
-            e = jk ? launch_stream_tick_jit(jk, items, (uint32_t)plan.items.size(), rec, strips, plan.SX, plan.SXp,
+            e = jk ? launch_stream_tick_jit(t ? jk.derived : jk.counting, items, (uint32_t)plan.items.size(), rec, strips, plan.SX, plan.SXp,
                                             plan.threads, ctx->stream, pdl, (int)t)
                    : launch_stream_tick((int)(d.flags & 7u), (int)s.rule.nterms, &s.rule, items,
                                         (uint32_t)plan.items.size(), rec, strips, plan.SX, plan.SXp, plan.threads,
                                         ctx->stream, pdl, (int)t);
     }
-    if (e == cudaSuccess && nticks) e = launch_fold_deferred(rec, tt, nticks, ctx->stream);
+    if (e == cudaSuccess && nticks) e = launch_fold_deferred(rec, tt, nticks, (bool)jk, ctx->stream);
     const uint4* last = strips + (uint64_t)(nticks & 1u) * nstrips;
     if (e == cudaSuccess) e = launch_strips_to_render(last, d_out, g, ctx->stream);
     if (e == cudaSuccess && d_skip) e = launch_render_skip(last, d_skip, g, ctx->stream);

@@ -8,9 +8,9 @@
 // from warp shuffles, y-neighbour column sums from a shared-memory exchange, z-neighbours
 // from the thread's rolling registers.
 //
-// Three march orders exist (`pipe`): grouped (2, the default: unrolled by four, every warp
-// waits on its slot's mbarrier), plain (0: one CTA barrier per plane) and software-pipelined
-// (1: a thread finishes plane k and starts plane k+1 between two barriers).
+// The march is unrolled by four so that exchange buffers and slot offsets are fixed within a
+// group; every warp waits on the mbarrier of the slot it reads, and one CTA barrier per plane
+// separates the y-exchange write from its reads.
 //
 // Ticks are chained with programmatic dependent launch: a tick's CTAs set up their shared
 // memory while the previous tick drains, then wait for it before touching the grid.
@@ -43,35 +43,24 @@ struct RuntimeRule {
     __device__ static DeviceRule rule() { return DeviceRule{}; }
 };
 
-template <int NB, int NT, bool PR, class Fixed>
+// kCountZero: count the cells that were 0 before the tick; a deferred-fold run may instead derive
+// them from the previous tick's population (all ticks after its first).
+template <int NB, int NT, bool PR, class Fixed, bool kCountZero = true>
 __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ items, StripSim* sims, uint4* pool,
-                                                 uint32_t sxp_log2, uint32_t pipe, int tick_arg,
-                                                 const DeviceRule& prule) {
+                                                 uint32_t sxp_log2, int tick_arg, const DeviceRule& prule) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ uint32_t s_skip;
+    __shared__ uint32_t s_state[2];  // done, tick (records that count their own ticks)
     __shared__ uint32_t red[32][11];
-    __shared__ bool s_last;
     const StreamItem it = items[blockIdx.x];
+    StripSim* sim = sims + it.sim;
     const uint32_t SXp = 1u << sxp_log2;
     const uint32_t rows = blockDim.x >> sxp_log2;  // incl. the two halo rows
-    uint64_t* bars;
-    {
-        const uint32_t SXc = sims[it.sim].SX;  // geometry is fixed for the run
-        bars = reinterpret_cast<uint64_t*>(reinterpret_cast<uint4*>(smem_raw) + (size_t)kRing * rows * SXc +
-                                           (size_t)kXch * rows * SXp);
-    }
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < kRing; s++) mbar_init(&bars[s], 1);
-        mbar_init_fence();
-    }
-    // Everything below reads the previous tick's results.
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    StripSim* sim = sims + it.sim;
-    if (threadIdx.x == 0) s_skip = sim->done;
-    __syncthreads();
-    if (s_skip) return;
-    asm volatile("griddepcontrol.launch_dependents;");
-
+    // A record's geometry, cell buffers and rule stay fixed while its simulation runs, so they
+    // are read while the previous tick drains, before griddepcontrol.wait. (A launch that may
+    // start early is never the first one after the record was written: those are launched
+    // without programmatic dependent launch.)
+    const uint32_t SX = sim->SX, X = sim->X, Y = sim->Y, Z = sim->Z;
+    const uint64_t buf0 = sim->buf[0], buf1 = sim->buf[1];
     DeviceRule lr;
     if constexpr (Fixed::kFixed) {
         lr = Fixed::rule();  // compile-time constants: every rule field folds into the logic
@@ -86,21 +75,46 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
         for (int t = 0; t < NT; t++) lr.terms[t] = g.terms[t];
     }
     const DeviceRule& R = (PR && !Fixed::kFixed) ? prule : lr;
-
-    const uint32_t SX = sim->SX, X = sim->X, Y = sim->Y, Z = sim->Z;
-    // A deferred-fold run (sim->deferred) passes the tick index; otherwise the record counts.
-    const uint32_t tick = tick_arg >= 0 ? (uint32_t)tick_arg : sim->tick;
-    const uint4* src = reinterpret_cast<const uint4*>(reinterpret_cast<unsigned char*>(pool) + sim->buf[tick & 1u]);
-    uint4* dst = reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(pool) + sim->buf[(tick + 1u) & 1u]);
     uint4* ring = reinterpret_cast<uint4*>(smem_raw);
     uint4* xch = ring + (size_t)kRing * rows * SX;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(xch + (size_t)kXch * rows * SXp);
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kRing; s++) mbar_init(&bars[s], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    // Everything below reads the previous tick's results.
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    uint32_t tick;
+    if (tick_arg >= 0) {
+        tick = (uint32_t)tick_arg;  // a deferred-fold run: the record is not updated between ticks
+    } else {
+        if (threadIdx.x == 0) {
+            s_state[0] = sim->done;
+            s_state[1] = sim->tick;
+        }
+        __syncthreads();
+        if (s_state[0]) return;
+        tick = s_state[1];
+    }
+    asm volatile("griddepcontrol.launch_dependents;");
+    const uint4* src =
+        reinterpret_cast<const uint4*>(reinterpret_cast<unsigned char*>(pool) + ((tick & 1u) ? buf1 : buf0));
+    uint4* dst = reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(pool) + ((tick & 1u) ? buf0 : buf1));
 
     const uint32_t sx = threadIdx.x & (SXp - 1u), yy = threadIdx.x >> sxp_log2;
     const int y = (int)it.y0 - 1 + (int)yy;
     const bool has = sx < SX && y >= 0 && y < (int)Y && yy < (uint32_t)it.ty + 2u;
     const bool outp = has && yy >= 1 && yy <= it.ty;
     const uint32_t valid = has ? strip_valid(sx, X) : 0u;
+    // x-neighbour bits travel by rotation inside the warp: lane - 1 (mod 32) holds the previous
+    // strip of the row or, for a row's first strip, the last lane of the previous row (or of the
+    // warp), which is a right edge or an absent strip; symmetrically for lane + 1. Each thread
+    // sends its alive plane with bit 31 cleared when it ends its row and bit 0 cleared when it
+    // starts it, so the bits that wrap across rows are zero (outside the grid is dead).
     const bool left_edge = sx == 0, right_edge = sx + 1 >= SX;
+    const uint32_t send_mask = (left_edge ? ~1u : ~0u) & (right_edge ? 0x7FFFFFFFu : ~0u);
+    const int lane_l = (int)((threadIdx.x + 31u) & 31u), lane_r = (int)((threadIdx.x + 1u) & 31u);
 
     // rows of the tile present in memory: [ylo, yhi)
     const int ylo = max((int)it.y0 - 1, 0), yhi = min((int)it.y0 + (int)it.ty + 1, (int)Y);
@@ -114,14 +128,14 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
     const int zfirst = down ? (int)it.z1 : (int)it.z0 - 1;  // plane of fetch 0
 
     // Thread 0 fills ring slot f % kRing with input plane f. A plane outside the grid is not
-    // copied; with `complete` set its slot's phase is completed by a plain arrive, so that every
-    // fetch advances its slot by exactly one phase (the grouped march relies on that).
-    auto issue = [&](int f, bool complete = false) {
+    // copied; its slot's phase is completed by a plain arrive instead, so that every fetch
+    // advances its slot by exactly one phase (the waits rely on that).
+    auto issue = [&](int f) {
         if (f >= nfetch) return;
         const int p = zfirst + f * zstep;
         const int s = f & (kRing - 1);
         if (p < 0 || p >= (int)Z) {
-            if (complete) mbar_arrive(&bars[s]);
+            mbar_arrive(&bars[s]);
             return;
         }
         uint4* slot = ring + (size_t)s * slot_stride + (size_t)slot_row0 * SX;
@@ -130,34 +144,21 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
         bulk_g2s(slot, g, tile_bytes, &bars[s]);
     };
     const uint32_t producer = 0;  // the thread that issues the plane copies
-    const bool grouped = pipe == 2u;
     if (threadIdx.x == producer) {
-        for (int f = 0; f < kRing; f++) issue(f, grouped);
+        for (int f = 0; f < kRing; f++) issue(f);
     }
 
     const uint4* my_ring = ring + (size_t)yy * SX + sx;
-    uint32_t phase = 0;  // bit s: parity to wait for on slot s
     uint32_t err = 0;
-    auto fetch = [&](int f) -> uint4 {
-        const int p = zfirst + f * zstep;
-        if (p < 0 || p >= (int)Z) return make_uint4(0, 0, 0, 0);
-        const int s = f & (kRing - 1);
-        if (!mbar_wait_bounded(&bars[s], (phase >> s) & 1u, kWaitLimitNs)) err = kErrWaitTimeout;
-        phase ^= 1u << s;
-        return has ? my_ring[(size_t)s * slot_stride] : make_uint4(0, 0, 0, 0);
-    };
     auto row_of = [&](uint4 st) -> Row {
         const uint32_t a = alive_plane(st, R);  // zero for absent strips: state 0 is never alive
-        uint32_t al = __shfl_up_sync(0xFFFFFFFFu, a, 1, SXp);
-        uint32_t ar = __shfl_down_sync(0xFFFFFFFFu, a, 1, SXp);
-        al = left_edge ? 0u : al;
-        ar = right_edge ? 0u : ar;
-        return make_row(a, al, ar);
+        const uint32_t v = a & send_mask;
+        return make_row(a, __shfl_sync(0xFFFFFFFFu, v, lane_l), __shfl_sync(0xFFFFFFFFu, v, lane_r));
     };
 
     using P = Partials<NB>;
     TickAcc acc;
-    acc.reset();
+    acc.reset(SX != 0u ? 1u : 0u);  // SX >= 1: a 1 the compiler cannot fold
     uint32_t xbits = 0u;
     uint4* my_x = xch + threadIdx.x;
     uint4* my_dst = dst + ((size_t)max(y, 0) * SX + sx);
@@ -165,158 +166,68 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
     const size_t xpar = (size_t)rows * SXp;
 
     int zo = zfirst + zstep;
-    if (grouped) {
-        // Grouped order: the plain order below, unrolled by kUnroll so that exchange buffers
-        // and slot offsets are fixed within a group and the plane rotation needs no register
-        // moves. Every warp waits for the copy of the plane it reads; fetch f is the
-        // (f / kRing)-th use of slot f % kRing, so the phase parity to wait for is (f / kRing) & 1.
-        auto read = [&](int f, int s) -> uint4 {  // s == f % kRing
-            const int p = zfirst + f * zstep;
-            if (f >= nfetch || (unsigned)p >= Z) return make_uint4(0, 0, 0, 0);
+    // Fetch f is the (f / kRing)-th use of slot f % kRing, so the phase parity to wait for is
+    // (f / kRing) & 1.
+    auto read = [&](int f, int s) -> uint4 {  // s == f % kRing
+        const int p = zfirst + f * zstep;
+        if (f >= nfetch || (unsigned)p >= Z) return make_uint4(0, 0, 0, 0);
+        if (!mbar_wait_bounded(&bars[s], (uint32_t)(f >> kRingLog2) & 1u, kWaitLimitNs)) err = kErrWaitTimeout;
+        return has ? my_ring[(size_t)s * slot_stride] : make_uint4(0, 0, 0, 0);
+    };
+    Row r_m = row_of(read(0, 0));
+    uint4 s_c = read(1, 1);
+    Row r_c = row_of(s_c);
+    __syncthreads();  // slots 0 and 1 consumed
+    if (threadIdx.x == producer) {
+        fence_proxy_async();
+        issue(kRing);
+        issue(kRing + 1);
+    }
+    // One plane: the next input plane's rows and column sums, the y-exchange, then the output
+    // strip. U: the plane's position in the unrolled group (selects the exchange buffer).
+    // `checked`: the fetch may lie outside the grid -- only the last plane's fetch can (fetch
+    // f <= L reads plane z0 - 1 + f, or z1 - f when marching down, inside [z0, z1)).
+    auto body = [&](int k, const int U, const bool checked) {
+        const int f = k + 2, s = f & (kRing - 1);
+        uint4 s_in;
+        if (checked) {
+            s_in = read(f, s);
+        } else {
             if (!mbar_wait_bounded(&bars[s], (uint32_t)(f >> kRingLog2) & 1u, kWaitLimitNs)) err = kErrWaitTimeout;
-            return has ? my_ring[(size_t)s * slot_stride] : make_uint4(0, 0, 0, 0);
-        };
-        Row r_m = row_of(read(0, 0));
-        uint4 s_c = read(1, 1);
-        Row r_c = row_of(s_c);
-        __syncthreads();  // slots 0 and 1 consumed
+            s_in = has ? my_ring[(size_t)s * slot_stride] : make_uint4(0, 0, 0, 0);
+        }
+        const Row r_p = row_of(s_in);
+        uint32_t pc[P::NC], ps[P::NS];
+        P::make(r_m, r_c, r_p, pc, ps);
+        uint4* xb = my_x + (size_t)(U & 1) * xpar;
+        *xb = pack_planes<P::NS>(ps);
+        __syncthreads();
         if (threadIdx.x == producer) {
             fence_proxy_async();
-            issue(kRing, true);
-            issue(kRing + 1, true);
+            issue(f + kRing);
         }
-        auto body = [&]<int U>(int k) {  // k % kUnroll == U
-            const uint4 s_in = read(k + 2, (k + 2) & (kRing - 1));
-            const Row r_p = row_of(s_in);
-            uint32_t pc[P::NC], ps[P::NS];
-            P::make(r_m, r_c, r_p, pc, ps);
-            uint4* xb = my_x + (size_t)(U & 1) * xpar;
-            *xb = pack_planes<P::NS>(ps);
-            __syncthreads();
-            if (threadIdx.x == producer) {
-                fence_proxy_async();
-                issue(k + 2 + kRing, true);
-            }
-            if (outp) {
-                const uint4 qm = *(xb - SXp), qp = *(xb + SXp);
-                const uint32_t psm[4] = {qm.x, qm.y, qm.z, qm.w}, psp[4] = {qp.x, qp.y, qp.z, qp.w};
-                uint32_t cnt[count_bits(NB)];
-                combine<NB>(pc, psm, psp, cnt);
-                my_dst[(size_t)zo * plane_stride] =
-                    update_strip<NB, NT>(s_c, r_c.a, cnt, valid, R, acc, xbits, (uint32_t)zo);
-            }
-            r_m = r_c;
-            r_c = r_p;
-            s_c = s_in;
-            zo += zstep;
-        };
-        static_assert(kUnroll == 4, "the grouped march is unrolled four times");
-        for (int k = 0; k < L; k += kUnroll) {
-            body.template operator()<0>(k);
-            if (k + 1 < L) body.template operator()<1>(k + 1);
-            if (k + 2 < L) body.template operator()<2>(k + 2);
-            if (k + 3 < L) body.template operator()<3>(k + 3);
-        }
-    } else if (!pipe) {
-        // Plain order: per plane, column sums -> barrier -> count, rule, update, store.
-        Row r_m = row_of(fetch(0));
-        uint4 s_c = fetch(1);
-        Row r_c = row_of(s_c);
-        __syncthreads();  // slots 0 and 1 consumed
-        if (threadIdx.x == 0) {
-            fence_proxy_async();
-            issue(kRing);
-            issue(kRing + 1);
-        }
-        for (int k = 0; k < L; k++) {
-            const uint4 s_in = fetch(k + 2);
-            const Row r_p = row_of(s_in);
-            uint32_t pc[P::NC], ps[P::NS];
-            P::make(r_m, r_c, r_p, pc, ps);
-            uint4* xb = my_x + (size_t)(k & 1) * xpar;
-            *xb = pack_planes<P::NS>(ps);
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                fence_proxy_async();
-                issue(k + 2 + kRing);
-            }
-            if (outp) {
-                const uint4 qm = *(xb - SXp), qp = *(xb + SXp);
-                const uint32_t psm[4] = {qm.x, qm.y, qm.z, qm.w}, psp[4] = {qp.x, qp.y, qp.z, qp.w};
-                uint32_t cnt[count_bits(NB)];
-                combine<NB>(pc, psm, psp, cnt);
-                my_dst[(size_t)zo * plane_stride] =
-                    update_strip<NB, NT>(s_c, r_c.a, cnt, valid, R, acc, xbits, (uint32_t)zo);
-            }
-            r_m = r_c;
-            r_c = r_p;
-            s_c = s_in;
-            zo += zstep;
-        }
-    } else {
-    // Software-pipelined order (see the file comment).
-    // prologue: rows of fetches 0..2 and the column sums of plane 0
-    Row r_a = row_of(fetch(0));          // plane before the first output
-    uint4 s_b = fetch(1);                 // first output plane
-    Row r_b = row_of(s_b);
-    uint4 s_c = fetch(2);
-    Row r_c = row_of(s_c);
-    uint32_t pc[P::NC];
-    {
-        uint32_t ps[P::NS];
-        P::make(r_a, r_b, r_c, pc, ps);
-        my_x[0] = pack_planes<P::NS>(ps);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        fence_proxy_async();
-        for (int f = kRing; f < kRing + 3; f++) issue(f);
-    }
-
-    for (int k = 0; k < L; k++) {
-        // (1) finish plane k: rows (a, b, c), centre state s_b, column sums pc, exchange slot k&1
-        uint4 nout;
-        {
-            // Only output rows (1 <= yy <= ty <= rows-2) read their y-neighbours: the halo rows'
-            // neighbours would lie outside the exchange buffer.
-            const uint4* xb = my_x + (size_t)(k & 1) * xpar;
-            uint4 qm = make_uint4(0, 0, 0, 0), qp = qm;
-            if (outp) {
-                qm = *(xb - SXp);
-                qp = *(xb + SXp);
-            }
+        if (outp) {
+            const uint4 qm = *(xb - SXp), qp = *(xb + SXp);
             const uint32_t psm[4] = {qm.x, qm.y, qm.z, qm.w}, psp[4] = {qp.x, qp.y, qp.z, qp.w};
             uint32_t cnt[count_bits(NB)];
             combine<NB>(pc, psm, psp, cnt);
-            nout = update_strip<NB, NT>(s_b, r_b.a, cnt, valid, R, acc, xbits, (uint32_t)zo, outp);
+            my_dst[(size_t)zo * plane_stride] =
+                update_strip<NB, NT, kCountZero>(s_c, r_c.a, cnt, valid, R, acc, xbits, (uint32_t)zo);
         }
-        // (2) start plane k+1: fetch k+3, rows (b, c, d), column sums into exchange slot (k+1)&1
-        const bool more = k + 1 < L;
-        uint4 s_d = make_uint4(0, 0, 0, 0);
-        Row r_d = r_c;
-        if (more) {
-            s_d = fetch(k + 3);
-            r_d = row_of(s_d);
-            uint32_t ps[P::NS];
-            P::make(r_b, r_c, r_d, pc, ps);
-            my_x[(size_t)((k + 1) & 1) * xpar] = pack_planes<P::NS>(ps);
-        }
-        if (outp) my_dst[(size_t)zo * plane_stride] = nout;
-        if (more) {
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                fence_proxy_async();
-                issue(k + 3 + kRing);
-            }
-        }
-        r_b = r_c;
-        r_c = r_d;
-        s_b = s_c;
-        s_c = s_d;
+        r_m = r_c;
+        r_c = r_p;
+        s_c = s_in;
         zo += zstep;
+    };
+    static_assert(kUnroll == 4, "the march is unrolled four times");
+    int k = 0;
+    for (; k + kUnroll < L; k += kUnroll) {  // every fetch inside the grid
+        body(k, 0, false);
+        body(k + 1, 1, false);
+        body(k + 2, 2, false);
+        body(k + 3, 3, false);
     }
-
-    }
+    for (; k < L; k++) body(k, k & 1, k + 1 == L);
 
     // ---- per-CTA reduction of the tick statistics
     uint32_t bx0 = 0xFFFFFFFFu, bx1 = 0u, by0 = 0xFFFFFFFFu, by1 = 0u;
@@ -336,13 +247,17 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
         for (int q = 7; q < 10; q++) v[q] = max(v[q], __shfl_xor_sync(0xFFFFFFFFu, v[q], o));
         v[10] |= __shfl_xor_sync(0xFFFFFFFFu, v[10], o);
     }
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     if (lane == 0) {
 #pragma unroll
         for (int q = 0; q < 11; q++) red[warp][q] = v[q];
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (warp != 0) return;
+    // Lane 0 of warp 0 folds the per-warp values (measured faster than a parallel fold by 11
+    // lanes); then lane q (< 11) applies column q to the record with one atomic -- 0..3 sums,
+    // 4..6 bounding-box minimum, 7..9 maximum, 10 error flags.
+    if (lane == 0) {
         const uint32_t nw = blockDim.x >> 5;
         for (uint32_t w = 1; w < nw; w++) {
             for (int q = 0; q < 4; q++) red[0][q] += red[w][q];
@@ -350,39 +265,29 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
             for (int q = 7; q < 10; q++) red[0][q] = max(red[0][q], red[w][q]);
             red[0][10] |= red[w][10];
         }
-        if (tick_arg >= 0) {
-            // deferred fold: add this CTA's totals to the tick's slot (no ticket, no fence:
-            // the next launch starts after this one has completed and flushed)
-            TickTotals* d = sim->deferred + tick;
-            if (red[0][0]) atomicAdd(&d->surv, red[0][0]);
-            if (red[0][1]) atomicAdd(&d->born, red[0][1]);
-            if (red[0][2]) atomicAdd(&d->zero, red[0][2]);
-            if (red[0][3]) {
-                atomicAdd(&d->pop, red[0][3]);
-                for (int q = 0; q < 3; q++) {
-                    atomicMax(&d->nbmin[q], ~red[0][4 + q]);
-                    atomicMax(&d->bmax[q], red[0][7 + q]);
-                }
-            }
-            if (red[0][10]) atomicOr(&sim->error, red[0][10]);
-            return;
-        }
-        if (red[0][0]) atomicAdd(&sim->acc_surv, red[0][0]);
-        if (red[0][1]) atomicAdd(&sim->acc_born, red[0][1]);
-        if (red[0][2]) atomicAdd(&sim->acc_zero, red[0][2]);
-        if (red[0][3]) {
-            atomicAdd(&sim->acc_pop, red[0][3]);
-            for (int q = 0; q < 3; q++) {
-                atomicMin(&sim->acc_bmin[q], red[0][4 + q]);
-                atomicMax(&sim->acc_bmax[q], red[0][7 + q]);
-            }
-        }
-        if (red[0][10]) atomicOr(&sim->error, red[0][10]);
-        __threadfence();
-        s_last = atomicAdd(&sim->ticket, 1u) == (it.dir_items >> 1) - 1u;
     }
-    __syncthreads();
-    if (threadIdx.x == 0 && s_last) {
+    __syncwarp();
+    const uint32_t x = red[0][lane < 11u ? lane : 10u];
+    const uint32_t pop = __shfl_sync(0xFFFFFFFFu, x, 3);
+    if (tick_arg >= 0) {
+        // deferred fold: add this CTA's totals to the tick's slot (no ticket, no fence: the next
+        // launch starts after this one has completed and flushed)
+        TickTotals* d = sim->deferred + tick;
+        if (lane < 4u && x) atomicAdd(&d->surv + lane, x);
+        if (lane >= 4u && lane < 7u && pop) atomicMax(&d->nbmin[lane - 4u], ~x);
+        if (lane >= 7u && lane < 10u && pop) atomicMax(&d->bmax[lane - 7u], x);
+        if (lane == 10u && x) atomicOr(&sim->error, x);
+        return;
+    }
+    if (lane < 4u && x) atomicAdd(&sim->acc_surv + lane, x);
+    if (lane >= 4u && lane < 7u && pop) atomicMin(&sim->acc_bmin[lane - 4u], x);
+    if (lane >= 7u && lane < 10u && pop) atomicMax(&sim->acc_bmax[lane - 7u], x);
+    if (lane == 10u && x) atomicOr(&sim->error, x);
+    __threadfence();  // each lane's update is visible before the ticket is taken
+    __syncwarp();
+    bool last = false;
+    if (lane == 0) last = atomicAdd(&sim->ticket, 1u) == (it.dir_items >> 1) - 1u;
+    if (__shfl_sync(0xFFFFFFFFu, last, 0) && lane == 0) {
         __threadfence();
         fold_tick(sim);
     }
