@@ -209,6 +209,48 @@ __device__ __forceinline__ void combine(const uint32_t* pc, const uint32_t* psm,
     add3<P::NC, P::NS, P::NS, count_bits(NB)>(pc, psm, psp, cnt);
 }
 
+// Column sums of the FEC neighbourhood kept in carry-save form: the column's three H summed by
+// two full adders and left unresolved, its sum (at most 9) being pc[0] + 2 (pc[1] + pc[2]) +
+// 4 pc[3]; combine resolves three such columns at once (4 + 16 logic operations per strip
+// against 8 + 15 for Partials<7> and combine<7>). Used by the rule-specialised tick kernels,
+// where it measured faster; the generic kernels measured slower with it and keep Partials<7>.
+struct MooreCarrySave {
+    static constexpr int NC = 4, NS = 4;
+    __device__ static void make(const Row& m, const Row& c, const Row& p, uint32_t* pc, uint32_t* ps) {
+        pc[0] = xor3(m.h0, c.h0, p.h0);  // weight 1
+        pc[1] = maj3(m.h0, c.h0, p.h0);  // weight 2
+        pc[2] = xor3(m.h1, c.h1, p.h1);  // weight 2
+        pc[3] = maj3(m.h1, c.h1, p.h1);  // weight 4
+#pragma unroll
+        for (int i = 0; i < 4; i++) ps[i] = pc[i];
+    }
+    // Three columns into the binary count (at most 27) with eight full adders and one half
+    // adder: the bits of each weight are reduced in threes and their carries passed up.
+    __device__ static void combine(const uint32_t* c, const uint32_t* m, const uint32_t* p, uint32_t* cnt) {
+        cnt[0] = xor3(c[0], m[0], p[0]);  // weight 1: 3 bits
+        const uint32_t c1 = maj3(c[0], m[0], p[0]);
+        const uint32_t sa = xor3(c[1], c[2], m[1]), ka = maj3(c[1], c[2], m[1]);  // weight 2: 6 bits + carry
+        const uint32_t sb = xor3(m[2], p[1], p[2]), kb = maj3(m[2], p[1], p[2]);
+        cnt[1] = xor3(sa, sb, c1);
+        const uint32_t kc = maj3(sa, sb, c1);
+        const uint32_t sd = xor3(c[3], m[3], p[3]), k1 = maj3(c[3], m[3], p[3]);  // weight 4: 3 bits + 3 carries
+        const uint32_t se = xor3(ka, kb, kc), k2 = maj3(ka, kb, kc);
+        cnt[2] = sd ^ se;
+        const uint32_t k3 = sd & se;
+        cnt[3] = xor3(k1, k2, k3);  // weight 8: 3 carries
+        cnt[4] = maj3(k1, k2, k3);  // weight 16
+    }
+};
+
+// The column-sum policy of a kernel: P::make and P::combine.
+template <int NB> struct BinaryColumns : Partials<NB> {
+    __device__ static void combine(const uint32_t* pc, const uint32_t* psm, const uint32_t* psp, uint32_t* cnt) {
+        cave::combine<NB>(pc, psm, psp, cnt);
+    }
+};
+template <int NB, bool kCarrySave> struct ColumnsFor { using type = BinaryColumns<NB>; };
+template <> struct ColumnsFor<7, true> { using type = MooreCarrySave; };
+
 // ---------------------------------------------------------------- state update + stats
 // acc + v as an integer multiply-add by `one`, so that the add issues on the FMA pipe instead of
 // the integer ALU, which the cell logic keeps busy. `one` must be 1 at run time in a way the

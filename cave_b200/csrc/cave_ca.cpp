@@ -473,7 +473,7 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
     const JitKernels jk = nticks ? jit_stream_kernel(jit_key(s.rule), jm, (uint64_t)g->X * g->Y * g->Z >= kJitMinCells)
                                  : JitKernels{};
     for (uint32_t t = 0; t < nticks && e == cudaSuccess; t++)
-        e = jk ? launch_stream_tick_jit(t ? jk.derived : jk.counting, ditems, (uint32_t)plan.items.size(), g->sim,
+        e = jk ? launch_stream_tick_jit(jk.pick(t == 0, plan.SX == plan.SXp), ditems, (uint32_t)plan.items.size(), g->sim,
                                         g->strips, plan.SX, plan.SXp, plan.threads, ctx->stream, true, (int)t)
                : launch_stream_tick((int)(d.flags & 7u), (int)s.rule.nterms, &s.rule, ditems,
                                     (uint32_t)plan.items.size(), g->sim, g->strips, plan.SX, plan.SXp, plan.threads,

@@ -55,21 +55,20 @@ struct JitRule {
     }
 };
 }  // namespace cave
-extern "C" __global__ void __launch_bounds__(1024)
-cave_stream_tick_jit(const cave::StreamItem* __restrict__ items, cave::StripSim* sims, uint4* pool,
-                     uint32_t sxp_log2, int tick_arg) {
-    cave::stream_tick_body<CAVE_JIT_NB, 0, false, cave::JitRule, true>(items, sims, pool, sxp_log2, tick_arg,
-                                                                      cave::DeviceRule{});
-}
-extern "C" __global__ void __launch_bounds__(1024)
-cave_stream_tick_jit_derived(const cave::StreamItem* __restrict__ items, cave::StripSim* sims, uint4* pool,
-                             uint32_t sxp_log2, int tick_arg) {
-    cave::stream_tick_body<CAVE_JIT_NB, 0, false, cave::JitRule, false>(items, sims, pool, sxp_log2, tick_arg,
-                                                                       cave::DeviceRule{});
-}
+#define CAVE_JIT_KERNEL(NAME, COUNT_ZERO, DENSE)                                                           \
+    extern "C" __global__ void __launch_bounds__(1024)                                                     \
+        NAME(const cave::StreamItem* __restrict__ items, cave::StripSim* sims, uint4* pool, uint32_t sxp_log2, \
+             int tick_arg) {                                                                               \
+        cave::stream_tick_body<CAVE_JIT_NB, 0, false, cave::JitRule, COUNT_ZERO, DENSE>(                    \
+            items, sims, pool, sxp_log2, tick_arg, cave::DeviceRule{});                                    \
+    }
+CAVE_JIT_KERNEL(cave_stream_tick_jit, true, false)
+CAVE_JIT_KERNEL(cave_stream_tick_jit_derived, false, false)
+CAVE_JIT_KERNEL(cave_stream_tick_jit_dense, true, true)
+CAVE_JIT_KERNEL(cave_stream_tick_jit_dense_derived, false, true)
 )cave_unit";
-const char* const kJitKernelName = "cave_stream_tick_jit";
-const char* const kJitDerivedName = "cave_stream_tick_jit_derived";
+const char* const kJitCounting[2] = {"cave_stream_tick_jit", "cave_stream_tick_jit_dense"};
+const char* const kJitDerived[2] = {"cave_stream_tick_jit_derived", "cave_stream_tick_jit_dense_derived"};
 
 struct Nvrtc {
     bool ok = false;
@@ -344,8 +343,10 @@ JitKernels jit_stream_kernel(const JitKey& k, JitMode mode, bool start) {
     }
     if (e->state != State::Compiled) return JitKernels{};
     cudaError_t err = cudaLibraryLoadData(&e->lib, e->cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
-    if (err == cudaSuccess) err = cudaLibraryGetKernel(&e->kern.counting, e->lib, kJitKernelName);
-    if (err == cudaSuccess) err = cudaLibraryGetKernel(&e->kern.derived, e->lib, kJitDerivedName);
+    for (int d = 0; d < 2 && err == cudaSuccess; d++) {
+        err = cudaLibraryGetKernel(&e->kern.counting[d], e->lib, kJitCounting[d]);
+        if (err == cudaSuccess) err = cudaLibraryGetKernel(&e->kern.derived[d], e->lib, kJitDerived[d]);
+    }
     if (err != cudaSuccess) {
         (void)cudaGetLastError();
         e->state = State::Failed;

@@ -37,10 +37,13 @@ constexpr uint64_t kJitMinCells = 1ull << 21;
 // The two specialised kernels of one key: `counting` counts every statistic; `derived` leaves
 // out the cells that were 0 before the tick, which a deferred fold derives from the previous
 // tick's population (every tick of a run after its first).
+// Each comes in two forms, indexed by `dense`: [1] for launches whose rows fill the lanes
+// (strips per row a power of two), [0] for any launch.
 struct JitKernels {
-    cudaKernel_t counting = nullptr;
-    cudaKernel_t derived = nullptr;
-    explicit operator bool() const { return counting != nullptr; }
+    cudaKernel_t counting[2] = {nullptr, nullptr};
+    cudaKernel_t derived[2] = {nullptr, nullptr};
+    explicit operator bool() const { return counting[0] != nullptr; }
+    cudaKernel_t pick(bool first_tick, bool dense) const { return first_tick ? counting[dense] : derived[dense]; }
 };
 
 // The specialised kernels for `k` if they are ready (loaded into the runtime), else empty. In

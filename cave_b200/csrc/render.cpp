@@ -91,7 +91,7 @@ cave_status cave_render_step(cave_ctx* ctx, const uint32_t* d_in, uint32_t* d_ou
         if (pad) e = launch_ghost_fill(strips + (uint64_t)(t & 1u) * nstrips, g, ctx->stream);
         const bool pdl = t > 0 && !pad;
         if (e == cudaSuccess)
-            e = jk ? launch_stream_tick_jit(t ? jk.derived : jk.counting, items, (uint32_t)plan.items.size(), rec, strips, plan.SX, plan.SXp,
+            e = jk ? launch_stream_tick_jit(jk.pick(t == 0, plan.SX == plan.SXp), items, (uint32_t)plan.items.size(), rec, strips, plan.SX, plan.SXp,
                                             plan.threads, ctx->stream, pdl, (int)t)
                    : launch_stream_tick((int)(d.flags & 7u), (int)s.rule.nterms, &s.rule, items,
                                         (uint32_t)plan.items.size(), rec, strips, plan.SX, plan.SXp, plan.threads,

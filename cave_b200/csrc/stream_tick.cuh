@@ -45,7 +45,9 @@ struct RuntimeRule {
 
 // kCountZero: count the cells that were 0 before the tick; a deferred-fold run may instead derive
 // them from the previous tick's population (all ticks after its first).
-template <int NB, int NT, bool PR, class Fixed, bool kCountZero = true>
+// kDense: the launch guarantees SX == SXp (every lane of a row holds a strip); ring positions of
+// rows outside the tile are then zeroed once and read like the others.
+template <int NB, int NT, bool PR, class Fixed, bool kCountZero = true, bool kDense = false>
 __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ items, StripSim* sims, uint4* pool,
                                                  uint32_t sxp_log2, int tick_arg, const DeviceRule& prule) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -149,6 +151,13 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
     }
 
     const uint4* my_ring = ring + (size_t)yy * SX + sx;
+    if constexpr (kDense) {
+        // rows the plane copies never write (outside the grid or the tile) read as dead cells
+        if (!has) {
+#pragma unroll
+            for (int s = 0; s < kRing; s++) const_cast<uint4*>(my_ring)[(size_t)s * slot_stride] = make_uint4(0, 0, 0, 0);
+        }
+    }
     uint32_t err = 0;
     auto row_of = [&](uint4 st) -> Row {
         const uint32_t a = alive_plane(st, R);  // zero for absent strips: state 0 is never alive
@@ -156,7 +165,7 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
         return make_row(a, __shfl_sync(0xFFFFFFFFu, v, lane_l), __shfl_sync(0xFFFFFFFFu, v, lane_r));
     };
 
-    using P = Partials<NB>;
+    using P = typename ColumnsFor<NB, Fixed::kFixed>::type;  // carry-save Moore columns when specialised
     TickAcc acc;
     acc.reset(SX != 0u ? 1u : 0u);  // SX >= 1: a 1 the compiler cannot fold
     uint32_t xbits = 0u;
@@ -194,7 +203,7 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
             s_in = read(f, s);
         } else {
             if (!mbar_wait_bounded(&bars[s], (uint32_t)(f >> kRingLog2) & 1u, kWaitLimitNs)) err = kErrWaitTimeout;
-            s_in = has ? my_ring[(size_t)s * slot_stride] : make_uint4(0, 0, 0, 0);
+            s_in = (kDense || has) ? my_ring[(size_t)s * slot_stride] : make_uint4(0, 0, 0, 0);
         }
         const Row r_p = row_of(s_in);
         uint32_t pc[P::NC], ps[P::NS];
@@ -210,7 +219,7 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
             const uint4 qm = *(xb - SXp), qp = *(xb + SXp);
             const uint32_t psm[4] = {qm.x, qm.y, qm.z, qm.w}, psp[4] = {qp.x, qp.y, qp.z, qp.w};
             uint32_t cnt[count_bits(NB)];
-            combine<NB>(pc, psm, psp, cnt);
+            P::combine(pc, psm, psp, cnt);
             my_dst[(size_t)zo * plane_stride] =
                 update_strip<NB, NT, kCountZero>(s_c, r_c.a, cnt, valid, R, acc, xbits, (uint32_t)zo);
         }
