@@ -10,8 +10,8 @@ namespace cave {
 
 constexpr int kRing = 8;      // plane slots in flight per CTA (power of two)
 constexpr int kRingLog2 = 3;
-constexpr int kUnroll = 4;    // the grouped march's unroll (divides kRing)
-static_assert((1 << kRingLog2) == kRing && kRing % kUnroll == 0, "ring geometry");
+constexpr int kUnroll = 6;    // the march's unroll: a multiple of the row rotation (3) and of the exchange buffers (2)
+static_assert((1 << kRingLog2) == kRing, "ring geometry");
 
 template <int N>
 __device__ __forceinline__ uint4 pack_planes(const uint32_t* p) {

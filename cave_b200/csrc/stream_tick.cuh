@@ -228,13 +228,15 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
         s_c = s_in;
         zo += zstep;
     };
-    static_assert(kUnroll == 4, "the march is unrolled four times");
+    static_assert(kUnroll == 6, "the march is unrolled six times");
     int k = 0;
     for (; k + kUnroll < L; k += kUnroll) {  // every fetch inside the grid
         body(k, 0, false);
         body(k + 1, 1, false);
         body(k + 2, 2, false);
         body(k + 3, 3, false);
+        body(k + 4, 4, false);
+        body(k + 5, 5, false);
     }
     for (; k < L; k++) body(k, k & 1, k + 1 == L);
 
