@@ -366,20 +366,23 @@ def sweep_workload(args, world, rank, local, pg):
             b.launch()
             b.results_array()
     barrier(pg, local)
-    kern_ms, tot_ms, wall, cats, ticks = [], [], [], None, 0
-    for _ in range(args.steps):
-        with make_batch() as b:
-            t0 = time.perf_counter()
-            b.add_sims_array(full, max_rule_bits=2)
-            b.launch()
-            res = b.results_array()
-            wall.append(time.perf_counter() - t0)
-            t = ctx.last_timing()
-            kern_ms.append(t.tick_ms)
-            tot_ms.append(t.total_ms)
-        cats = np.bincount(res["category"], minlength=3)
-        ticks = int(res["info"][:, 2].sum())
-    barrier(pg, local)
+    kern_ms, tot_ms, wall, cats, ticks, launches = [], [], [], None, 0, 0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            with make_batch() as b:
+                t0 = time.perf_counter()
+                b.add_sims_array(full, max_rule_bits=2)
+                b.launch()
+                res = b.results_array()
+                wall.append(time.perf_counter() - t0)
+                t = ctx.last_timing()
+                kern_ms.append(t.tick_ms)
+                tot_ms.append(t.total_ms)
+                launches += t.launches
+            cats = np.bincount(res["category"], minlength=3)
+            ticks = int(res["info"][:, 2].sum())
+        barrier(pg, local)
+    clocks = clk.summary()
     n_all = sum_over_ranks(pg, local, float(full.size))
     kern = max_over_ranks(pg, local, sum(kern_ms) / len(kern_ms))
     tot = max_over_ranks(pg, local, sum(tot_ms) / len(tot_ms))
@@ -414,7 +417,8 @@ def sweep_workload(args, world, rank, local, pg):
         "batched_over_plain": (sims_s / plain["best_sims_per_s"]) if plain else None,
         "e2e": {"value": n_all / (tot / 1e3), "unit": "sims/s", "h2d_bytes_per_step": int(full.size * 16),
                 "d2h_bytes_per_step": int(full.size * cb.SIM_RESULT_DTYPE.itemsize)},
-        "gpu_launches": 4 * args.steps,
+        "gpu_launches": int(sum_over_ranks(pg, local, launches)),
+        "clocks": clocks,
     }
     ctx.close()
     return line
@@ -482,21 +486,24 @@ def uneven_workload(args, world, rank, local, pg):
     tune_wall = time.perf_counter() - t0
     barrier(pg, local)
     kern_ms, tot_ms, wall = [], [], []
-    updates = 0
-    for _ in range(args.steps):
-        with make_batch(mine, autotune) as b:
-            w0 = time.perf_counter()
-            b.launch()
-            res = b.results_array()
-            wall.append(time.perf_counter() - w0)
-            t = ctx.last_timing()
-            kern_ms.append(t.tick_ms)
-            tot_ms.append(t.total_ms)
-            plan = b.plan()
-        vol = np.array([s["edge"] ** 3 for s in mine], dtype=np.int64)
-        updates = int((res["info"][:, 2].astype(np.int64) * vol).sum())
-        assert int(res["error"].max(initial=0)) == 0
-    barrier(pg, local)
+    updates, launches = 0, 0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            with make_batch(mine, autotune) as b:
+                w0 = time.perf_counter()
+                b.launch()
+                res = b.results_array()
+                wall.append(time.perf_counter() - w0)
+                t = ctx.last_timing()
+                kern_ms.append(t.tick_ms)
+                tot_ms.append(t.total_ms)
+                launches += t.launches
+                plan = b.plan()
+            vol = np.array([s["edge"] ** 3 for s in mine], dtype=np.int64)
+            updates = int((res["info"][:, 2].astype(np.int64) * vol).sum())
+            assert int(res["error"].max(initial=0)) == 0
+        barrier(pg, local)
+    clocks = clk.summary()
     kern = max_over_ranks(pg, local, sum(kern_ms) / len(kern_ms))
     tot = max_over_ranks(pg, local, sum(tot_ms) / len(tot_ms))
     n_all = sum_over_ranks(pg, local, float(len(mine)))
@@ -536,6 +543,8 @@ def uneven_workload(args, world, rank, local, pg):
         "e2e": {"value": n_all / (tot / 1e3), "unit": "sims/s", "h2d_bytes_per_step": int(len(mine) * 40),
                 "d2h_bytes_per_step": int(len(mine) * cb.SIM_RESULT_DTYPE.itemsize)},
         "host_wall_s_per_step": sum(wall) / len(wall),
+        "gpu_launches": int(sum_over_ranks(pg, local, launches)),
+        "clocks": clocks,
     }
     ctx.close()
     return line
@@ -609,8 +618,9 @@ def serve_workload(args, world, rank, local, pg):
             srv.wait(srv.submit(r), 600.0)
         for rid in srv.poll():
             pass
-    with cb.Server(ctx, hbm_budget=budget) as srv:
+    with cb.Server(ctx, hbm_budget=budget) as srv, ClockSampler(local) as clk:
         span_served, lat, st_served = run(srv, True)
+    clocks = clk.summary()
     with cb.Server(ctx, hbm_budget=budget) as srv:
         span_off, _, st_off = run(srv, False)
 
@@ -634,6 +644,8 @@ def serve_workload(args, world, rank, local, pg):
         "served_span_s": span_served, "offline_span_s": span_off, "peak_hbm_bytes": st_served.peakBytes,
         "tick_launches": st_served.tickLaunches, "resident_launches": st_served.residentLaunches,
         "rounds": st_served.rounds,
+        "gpu_launches": int(st_served.tickLaunches + st_served.residentLaunches + st_served.rounds),
+        "clocks": clocks,
         "e2e": {"value": served_ups, "unit": "cell-updates/s", "h2d_bytes_per_step": int(total_sims * 72),
                 "d2h_bytes_per_step": int(total_sims * cb.SIM_RESULT_DTYPE.itemsize)},
     }
