@@ -277,7 +277,9 @@ struct TickAcc {  // per-thread accumulators for one tick
 // xbits accumulates the OR of the strip's non-zero masks (its x-extent). The statistics are
 // accumulated only when `count` is set (strips this thread owns, not halo copies); cells that
 // were 0 only with kCountZero (a caller may derive them from the previous tick's population).
-template <int NB, int NT, bool kCountZero = true>
+// kFullRange: the rule's alive state is 15 (all four planes set; a compile-time fact of the
+// specialised kernels), which allows the shorter update below.
+template <int NB, int NT, bool kCountZero = true, bool kFullRange = false>
 __device__ __forceinline__ uint4 update_strip(uint4 s, uint32_t a, const uint32_t* cnt, uint32_t valid,
                                               const DeviceRule& r, TickAcc& acc, uint32_t& xbits, uint32_t z,
                                               bool count = true) {
@@ -287,20 +289,32 @@ __device__ __forceinline__ uint4 update_strip(uint4 s, uint32_t a, const uint32_
     const uint32_t zero = ~nz & valid;
     const uint32_t sv = a & hs;
     const uint32_t bn = zero & hb;
-    const uint32_t set = sv | bn;
-    // d = s - 1 for non-zero cells, 0 for zero cells (borrow chain masked by nz); then each
-    // plane is set ? bit of maxcs : d (one 3-input select per plane)
     const uint32_t b2 = ~s.x & ~s.y;
     const uint32_t b3 = b2 & ~s.z;
-    const uint32_t d0 = nz & ~s.x;
-    const uint32_t d1 = nz & ~(s.y ^ s.x);
-    const uint32_t d2 = nz & (s.z ^ b2);
-    const uint32_t d3 = nz & (s.w ^ b3);
     uint4 n;
-    n.x = (set & r.m[0]) | (~set & d0);
-    n.y = (set & r.m[1]) | (~set & d1);
-    n.z = (set & r.m[2]) | (~set & d2);
-    n.w = (set & r.m[3]) | (~set & d3);
+    if constexpr (kFullRange) {
+        // Alive state 15. A born cell (state 0) becomes 15 = 0 - 1 in four bits, so the borrow
+        // chain of the decrement runs on every cell of t = non-zero or born; a surviving cell
+        // (15) decrements to 14 and gets its low bit back from sv; every other cell is
+        // s - 1, or stays 0 outside t.
+        const uint32_t t = nz | bn;
+        n.x = sv | (t & ~s.x);
+        n.z = t & (s.z ^ b2);
+        n.w = t & (s.w ^ b3);
+        n.y = (s.x & s.y) | (~s.x & ~s.y & t);
+    } else {
+        // d = s - 1 for non-zero cells, 0 for zero cells (borrow chain masked by nz); then each
+        // plane is set ? bit of maxcs : d (one 3-input select per plane)
+        const uint32_t set = sv | bn;
+        const uint32_t d0 = nz & ~s.x;
+        const uint32_t d1 = nz & ~(s.y ^ s.x);
+        const uint32_t d2 = nz & (s.z ^ b2);
+        const uint32_t d3 = nz & (s.w ^ b3);
+        n.x = (set & r.m[0]) | (~set & d0);
+        n.y = (set & r.m[1]) | (~set & d1);
+        n.z = (set & r.m[2]) | (~set & d2);
+        n.w = (set & r.m[3]) | (~set & d3);
+    }
     if (count) {
         acc.surviving = mad_add(acc.surviving, __popc(sv), acc.one);
         acc.born = mad_add(acc.born, __popc(bn), acc.one);

@@ -42,6 +42,7 @@ const char* const kJitUnit = R"cave_unit(
 namespace cave {
 struct JitRule {
     static constexpr bool kFixed = true;
+    static constexpr bool kFullRange = CAVE_JIT_MAXCS == 15u;
     __device__ static DeviceRule rule() {
         DeviceRule r{};
         r.maxcs = CAVE_JIT_MAXCS;

@@ -40,6 +40,7 @@ namespace cave {
 // Fixed-rule policy of the library's own kernels: the rule is read at run time.
 struct RuntimeRule {
     static constexpr bool kFixed = false;
+    static constexpr bool kFullRange = false;  // alive state known to be 15
     __device__ static DeviceRule rule() { return DeviceRule{}; }
 };
 
@@ -221,7 +222,8 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
             uint32_t cnt[count_bits(NB)];
             P::combine(pc, psm, psp, cnt);
             my_dst[(size_t)zo * plane_stride] =
-                update_strip<NB, NT, kCountZero>(s_c, r_c.a, cnt, valid, R, acc, xbits, (uint32_t)zo);
+                update_strip<NB, NT, kCountZero, Fixed::kFullRange>(s_c, r_c.a, cnt, valid, R, acc, xbits,
+                                                                      (uint32_t)zo);
         }
         r_m = r_c;
         r_c = r_p;
