@@ -279,7 +279,11 @@ struct TickAcc {  // per-thread accumulators for one tick
 // were 0 only with kCountZero (a caller may derive them from the previous tick's population).
 // kFullRange: the rule's alive state is 15 (all four planes set; a compile-time fact of the
 // specialised kernels), which allows the shorter update below.
-template <int NB, int NT, bool kCountZero = true, bool kFullRange = false>
+// kPop: where the population and bounding box come from -- kPopOutput: the strip's new state
+// (the tick's own); kPopInput: its current state, i.e. the previous tick's result, whose
+// non-zero mask the update computes anyway; kPopNone: not counted.
+enum : int { kPopNone = 0, kPopOutput = 1, kPopInput = 2 };
+template <int NB, int NT, bool kCountZero = true, bool kFullRange = false, int kPop = kPopOutput>
 __device__ __forceinline__ uint4 update_strip(uint4 s, uint32_t a, const uint32_t* cnt, uint32_t valid,
                                               const DeviceRule& r, TickAcc& acc, uint32_t& xbits, uint32_t z,
                                               bool count = true) {
@@ -319,12 +323,14 @@ __device__ __forceinline__ uint4 update_strip(uint4 s, uint32_t a, const uint32_
         acc.surviving = mad_add(acc.surviving, __popc(sv), acc.one);
         acc.born = mad_add(acc.born, __popc(bn), acc.one);
         if constexpr (kCountZero) acc.zero = mad_add(acc.zero, __popc(zero), acc.one);
-        const uint32_t nn = n.x | n.y | n.z | n.w;
-        acc.population = mad_add(acc.population, __popc(nn), acc.one);
-        xbits |= nn;
-        const bool any = nn != 0u;
-        acc.zmin = any ? min(acc.zmin, z) : acc.zmin;
-        acc.zmax = any ? max(acc.zmax, z) : acc.zmax;
+        if constexpr (kPop != kPopNone) {
+            const uint32_t nn = kPop == kPopInput ? nz : (n.x | n.y | n.z | n.w);
+            acc.population = mad_add(acc.population, __popc(nn), acc.one);
+            xbits |= nn;
+            const bool any = nn != 0u;
+            acc.zmin = any ? min(acc.zmin, z) : acc.zmin;
+            acc.zmax = any ? max(acc.zmax, z) : acc.zmax;
+        }
     }
     return n;
 }

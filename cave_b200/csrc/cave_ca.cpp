@@ -478,6 +478,9 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
                : launch_stream_tick((int)(d.flags & 7u), (int)s.rule.nterms, &s.rule, ditems,
                                     (uint32_t)plan.items.size(), g->sim, g->strips, plan.SX, plan.SXp, plan.threads,
                                     ctx->stream, true, (int)t);
+    if (e == cudaSuccess && nticks && jk)  // the last tick's population comes from the final grid
+        e = launch_strip_stats(g->strips + (uint64_t)(nticks & 1u) * nstrips, g->Y, g->Z, plan.SX, dtt + (nticks - 1),
+                               (uint32_t)ctx->sm_count, ctx->stream);
     if (e == cudaSuccess && nticks) e = launch_fold_deferred(g->sim, dtt, nticks, (bool)jk, ctx->stream);
     record(ctx, 3);
     // Raw stepping never stops early, so the result is in copy (nticks & 1).
@@ -497,7 +500,7 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
     cudaFree(ditems);
     cudaFree(dtt);
     if (e != cudaSuccess) return check_cuda(ctx, e, "cave_run");
-    finish_timing(ctx, nticks, nticks + 3, true);
+    finish_timing(ctx, nticks, nticks + (jk ? 4 : 3), true);
     if (back.error & kErrWaitTimeout) return set_error(ctx, CAVE_ERR_TIMEOUT, "streaming kernel: bulk-copy wait timed out");
     if (back.error) return set_error(ctx, CAVE_ERR_INTERNAL, "streaming kernel raised an error flag");
     if (back.tick != nticks) return set_error(ctx, CAVE_ERR_INTERNAL, "streaming run stopped early");

@@ -34,9 +34,12 @@ inline JitKey jit_key(const DeviceRule& r) { return JitKey{r.flags & 7u, r.maxcs
 // Grids at least this large (cells) start a background compile in async mode.
 constexpr uint64_t kJitMinCells = 1ull << 21;
 
-// The two specialised kernels of one key: `counting` counts every statistic; `derived` leaves
-// out the cells that were 0 before the tick, which a deferred fold derives from the previous
-// tick's population (every tick of a run after its first).
+// The two specialised kernels of one key, both for deferred-fold runs: `counting` (a run's first
+// tick) counts the surviving, born and formerly-zero cells but not the population; `derived`
+// (every later tick) counts the surviving and born cells and the population and bounding box of
+// its input, i.e. of the previous tick, into that tick's slot. The fold derives the zero cells
+// from the previous population; a pass over the final grid (launch_strip_stats) supplies the
+// last tick's population and bounding box.
 // Each comes in two forms, indexed by `dense`: [1] for launches whose rows fill the lanes
 // (strips per row a power of two), [0] for any launch.
 struct JitKernels {

@@ -89,6 +89,9 @@ cudaError_t launch_render_skip(const uint4* strips, uint32_t* skip, const Render
 cudaError_t launch_stream_tick(int nb, int nt, const DeviceRule* param_rule, const StreamItem* items,
                                uint32_t n_items, StripSim* sims, uint4* pool, uint32_t SX, uint32_t SXp,
                                uint32_t threads, cudaStream_t st, bool pdl = true, int tick_arg = -1);
+// Population and bounding box of a strip grid (SX strips per row), added to `slot`.
+cudaError_t launch_strip_stats(const uint4* strips, uint32_t Y, uint32_t Z, uint32_t SX, TickTotals* slot,
+                               uint32_t sm_count, cudaStream_t st);
 // After the last tick of a deferred-fold run: per-tick statistics and the record's GridInfo.
 // derive_zero: ticks after the first did not count their zero cells (volume - previous population).
 cudaError_t launch_fold_deferred(StripSim* sim, const TickTotals* tt, uint32_t nticks, bool derive_zero,

@@ -96,6 +96,64 @@ __global__ void __launch_bounds__(256) k_fold_deferred(StripSim* sim, const Tick
     }
 }
 
+// Population and bounding box of a whole strip grid, added to one tick slot: the last tick of a
+// deferred-fold run whose ticks count their input's (every tick's but the last comes from the
+// tick after it). Cells past X are 0 in the strip layout.
+__global__ void __launch_bounds__(256) k_strip_stats(const uint4* __restrict__ strips, uint32_t Y, uint32_t Z,
+                                                     uint32_t SX, TickTotals* slot) {
+    __shared__ uint32_t red[8][7];
+    uint32_t v[7] = {0u, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u};  // pop, min xyz, max xyz
+    const uint64_t n = (uint64_t)SX * Y * Z;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint4 st = strips[i];
+        const uint32_t nz = st.x | st.y | st.z | st.w;
+        if (!nz) continue;
+        const uint32_t sx = (uint32_t)(i % SX);
+        const uint64_t row = i / SX;
+        const uint32_t y = (uint32_t)(row % Y), z = (uint32_t)(row / Y);
+        v[0] += __popc(nz);
+        v[1] = min(v[1], sx * 32u + (uint32_t)(__ffs(nz) - 1));
+        v[4] = max(v[4], sx * 32u + 31u - (uint32_t)__clz(nz));
+        v[2] = min(v[2], y);
+        v[5] = max(v[5], y);
+        v[3] = min(v[3], z);
+        v[6] = max(v[6], z);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v[0] += __shfl_xor_sync(0xFFFFFFFFu, v[0], o);
+#pragma unroll
+        for (int q = 1; q < 4; q++) v[q] = min(v[q], __shfl_xor_sync(0xFFFFFFFFu, v[q], o));
+#pragma unroll
+        for (int q = 4; q < 7; q++) v[q] = max(v[q], __shfl_xor_sync(0xFFFFFFFFu, v[q], o));
+    }
+    const uint32_t warp = threadIdx.x >> 5;
+    if ((threadIdx.x & 31u) == 0) {
+        for (int q = 0; q < 7; q++) red[warp][q] = v[q];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (uint32_t w = 1; w < (blockDim.x >> 5); w++) {
+            red[0][0] += red[w][0];
+            for (int q = 1; q < 4; q++) red[0][q] = min(red[0][q], red[w][q]);
+            for (int q = 4; q < 7; q++) red[0][q] = max(red[0][q], red[w][q]);
+        }
+        if (red[0][0]) {
+            atomicAdd(&slot->pop, red[0][0]);
+            for (int q = 0; q < 3; q++) {
+                atomicMax(&slot->nbmin[q], ~red[0][1 + q]);
+                atomicMax(&slot->bmax[q], red[0][4 + q]);
+            }
+        }
+    }
+}
+
+cudaError_t launch_strip_stats(const uint4* strips, uint32_t Y, uint32_t Z, uint32_t SX, TickTotals* slot,
+                               uint32_t sm_count, cudaStream_t st) {
+    k_strip_stats<<<sm_count * 4u, 256, 0, st>>>(strips, Y, Z, SX, slot);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_fold_deferred(StripSim* sim, const TickTotals* tt, uint32_t nticks, bool derive_zero,
                                  cudaStream_t st) {
     k_fold_deferred<<<1, 256, 0, st>>>(sim, tt, nticks, derive_zero ? 1u : 0u);

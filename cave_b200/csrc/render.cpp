@@ -97,6 +97,9 @@ cave_status cave_render_step(cave_ctx* ctx, const uint32_t* d_in, uint32_t* d_ou
                                         (uint32_t)plan.items.size(), rec, strips, plan.SX, plan.SXp, plan.threads,
                                         ctx->stream, pdl, (int)t);
     }
+    if (e == cudaSuccess && nticks && jk)  // the last tick's population comes from the final grid
+        e = launch_strip_stats(strips + (uint64_t)(nticks & 1u) * nstrips, g.Yp, g.Zp, g.SX, tt + (nticks - 1),
+                               (uint32_t)ctx->sm_count, ctx->stream);
     if (e == cudaSuccess && nticks) e = launch_fold_deferred(rec, tt, nticks, (bool)jk, ctx->stream);
     const uint4* last = strips + (uint64_t)(nticks & 1u) * nstrips;
     if (e == cudaSuccess) e = launch_strips_to_render(last, d_out, g, ctx->stream);

@@ -48,7 +48,11 @@ struct RuntimeRule {
 // them from the previous tick's population (all ticks after its first).
 // kDense: the launch guarantees SX == SXp (every lane of a row holds a strip); ring positions of
 // rows outside the tile are then zeroed once and read like the others.
-template <int NB, int NT, bool PR, class Fixed, bool kCountZero = true, bool kDense = false>
+// kPop (deferred-fold runs only; see update_strip): kPopInput counts the population and bounding
+// box of the tick's input into the previous tick's slot, kPopNone leaves them out (the first
+// tick of such a run; a pass over the final grid supplies the last tick's).
+template <int NB, int NT, bool PR, class Fixed, bool kCountZero = true, bool kDense = false,
+          int kPop = kPopOutput>
 __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ items, StripSim* sims, uint4* pool,
                                                  uint32_t sxp_log2, int tick_arg, const DeviceRule& prule) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -222,8 +226,8 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
             uint32_t cnt[count_bits(NB)];
             P::combine(pc, psm, psp, cnt);
             my_dst[(size_t)zo * plane_stride] =
-                update_strip<NB, NT, kCountZero, Fixed::kFullRange>(s_c, r_c.a, cnt, valid, R, acc, xbits,
-                                                                      (uint32_t)zo);
+                update_strip<NB, NT, kCountZero, Fixed::kFullRange, kPop>(s_c, r_c.a, cnt, valid, R, acc,
+                                                                            xbits, (uint32_t)zo);
         }
         r_m = r_c;
         r_c = r_p;
@@ -286,9 +290,13 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
         // deferred fold: add this CTA's totals to the tick's slot (no ticket, no fence: the next
         // launch starts after this one has completed and flushed)
         TickTotals* d = sim->deferred + tick;
-        if (lane < 4u && x) atomicAdd(&d->surv + lane, x);
-        if (lane >= 4u && lane < 7u && pop) atomicMax(&d->nbmin[lane - 4u], ~x);
-        if (lane >= 7u && lane < 10u && pop) atomicMax(&d->bmax[lane - 7u], x);
+        TickTotals* dp = kPop == kPopInput ? d - 1 : d;  // the slot the population belongs to
+        if (lane < 3u && x) atomicAdd(&d->surv + lane, x);
+        if (kPop != kPopNone) {
+            if (lane == 3u && x) atomicAdd(&dp->pop, x);
+            if (lane >= 4u && lane < 7u && pop) atomicMax(&dp->nbmin[lane - 4u], ~x);
+            if (lane >= 7u && lane < 10u && pop) atomicMax(&dp->bmax[lane - 7u], x);
+        }
         if (lane == 10u && x) atomicOr(&sim->error, x);
         return;
     }
