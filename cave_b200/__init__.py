@@ -193,6 +193,7 @@ _SIGS = {
     "cave_prepare_rule": (i32, [ctypes.c_void_p, P(SimParams), P(u64), u32, u32]),
     "cave_jit_compile": (i32, [P(SimParams), P(u64), u32, u32, ctypes.c_char_p, ctypes.c_size_t]),
     "cave_jit_stats": (None, [P(u32), P(u64)]),
+    "cave_jit_compile_async": (i32, [P(SimParams), P(u64), u32, u32]),
     "cave_manager_update": (None, [P(GridSnapshot), P(GridInfo), P(SimParams), u64, u64, u32, P(GridInfo),
                                    P(SimParams)]),
     "cave_enumerate_valid_bitmasks": (u64, [u32, u32, P(u64), u64]),
@@ -233,6 +234,14 @@ def jit_compile(params: "SimParams", valid=None, max_rule_bits=0):
     rc = lib().cave_jit_compile(ctypes.byref(params), _u64p(v), 0 if v is None else v.size, max_rule_bits, buf,
                                 len(buf))
     return rc == 0, buf.value.decode(errors="replace")
+
+
+def jit_compile_async(params: "SimParams", valid=None, max_rule_bits=0):
+    """Starts compiling the rule-specialised tick kernel in the background (no device)."""
+    v = None if valid is None else np.ascontiguousarray(valid, dtype=np.uint64)
+    rc = lib().cave_jit_compile_async(ctypes.byref(params), _u64p(v), 0 if v is None else v.size, max_rule_bits)
+    if rc != 0:
+        raise CaveError(rc, "cave_jit_compile_async")
 
 
 def jit_stats():

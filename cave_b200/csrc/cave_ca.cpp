@@ -376,6 +376,15 @@ cave_status cave_prepare_rule(cave_ctx* ctx, const cave_sim_params* params, cons
     return set_error(ctx, CAVE_ERR_INTERNAL, "rule-specialised kernel unavailable: " + log.substr(0, 2000));
 }
 
+cave_status cave_jit_compile_async(const cave_sim_params* params, const uint64_t* validBitmasks, uint32_t nValid,
+                                   uint32_t maxRuleBits) {
+    if (!params) return CAVE_ERR_INVALID_ARG;
+    DecodedRule d;
+    if (!decode_params(*params, validBitmasks, nValid, maxRuleBits, d)) return CAVE_ERR_INVALID_ARG;
+    if (jit_mode() != JitMode::Off) jit_compile_async(jit_key(make_device_rule(d)));
+    return CAVE_OK;
+}
+
 cave_status cave_jit_compile(const cave_sim_params* params, const uint64_t* validBitmasks, uint32_t nValid,
                              uint32_t maxRuleBits, char* log, size_t log_size) {
     if (!params) return CAVE_ERR_INVALID_ARG;

@@ -312,6 +312,49 @@ Registry& registry() {
     return r;
 }
 
+// NVRTC sets up static state of its own (and loads its builtins library) during its first
+// compile, and registers exit-time teardown for it then. A compile still running in the worker
+// when that teardown runs crashes the process. So before the worker starts, the calling thread
+// loads NVRTC and compiles an empty kernel, and only then registers join_worker_at_exit: exit
+// handlers run in reverse order of registration, so the worker is joined before NVRTC's state
+// is torn down.
+void prime_nvrtc() {
+    Nvrtc& n = nvrtc();
+    if (!n.ok) return;
+    nvrtcProgram prog = nullptr;
+    if (n.create(&prog, "extern \"C\" __global__ void cave_prime() {}", "cave_prime.cu", 0, nullptr, nullptr) !=
+        NVRTC_SUCCESS)
+        return;
+    const char* opts[] = {"--gpu-architecture=sm_100a"};
+    n.compile(prog, 1, opts);
+    n.destroy(&prog);
+}
+
+void join_worker_at_exit() {
+    Registry& R = registry();
+    {
+        std::lock_guard<std::mutex> g(R.mu);
+        R.stop = true;
+        R.queue.clear();
+    }
+    R.cv.notify_all();
+    if (R.worker.joinable()) R.worker.join();
+}
+
+// Queues k for the background compile (starting the worker on first use). Called with R.mu held.
+void queue_compile(Registry& R, const JitKey& k) {
+    Entry& e = R.entries[key_of(k)];
+    if (e.state != State::None || R.stop) return;
+    e.state = State::Queued;
+    R.queue.push_back(k);
+    if (!R.worker.joinable()) {
+        prime_nvrtc();
+        std::atexit(join_worker_at_exit);
+        R.worker = std::thread([&R] { R.run(); });
+    }
+    R.cv.notify_all();
+}
+
 std::atomic<uint32_t> g_loaded{0};
 std::atomic<uint64_t> g_launches{0};
 
@@ -336,11 +379,7 @@ JitKernels jit_stream_kernel(const JitKey& k, JitMode mode, bool start) {
         R.compile_now(lk, k);
         e = &R.entries[key_of(k)];
     } else if (e->state == State::None) {
-        if (!start) return JitKernels{};
-        e->state = State::Queued;
-        R.queue.push_back(k);
-        if (!R.worker.joinable()) R.worker = std::thread([&R] { R.run(); });
-        R.cv.notify_all();
+        if (start) queue_compile(R, k);
         return JitKernels{};
     }
     if (e->state != State::Compiled) return JitKernels{};
@@ -361,6 +400,12 @@ JitKernels jit_stream_kernel(const JitKey& k, JitMode mode, bool start) {
     e->state = State::Loaded;
     g_loaded.fetch_add(1, std::memory_order_relaxed);
     return e->kern;
+}
+
+void jit_compile_async(const JitKey& k) {
+    Registry& R = registry();
+    std::lock_guard<std::mutex> lk(R.mu);
+    queue_compile(R, k);
 }
 
 bool jit_compile(const JitKey& k, std::string* log) {

@@ -54,6 +54,9 @@ struct JitKernels {
 // is set. A key whose compile failed stays on the generic kernel.
 JitKernels jit_stream_kernel(const JitKey& k, JitMode mode, bool start);
 
+// Queues `k` for the background compile (no device needed; returns at once).
+void jit_compile_async(const JitKey& k);
+
 // Compiles the kernel for `k` into the caches (no device needed). Returns false with the
 // compiler's log (or the reason NVRTC is unavailable) in *log.
 bool jit_compile(const JitKey& k, std::string* log);

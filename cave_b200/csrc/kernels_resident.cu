@@ -60,7 +60,13 @@ __global__ void __launch_bounds__(1024) k_resident(ResLaunch P, const ResSim* __
     const bool in_seg = seg < P.nseg;
     const bool has = in_seg && sx < SX;
     const uint32_t valid = has ? strip_valid(sx, X) : 0u;
+    // x-neighbour bits by rotation inside the warp (as in the streaming kernel): lane - 1 (mod 32)
+    // of a row's first strip is the last lane of the previous row, segment or warp -- a right
+    // edge or an absent strip -- and each thread sends its alive plane with the bits that would
+    // wrap across rows cleared.
     const bool left_edge = sx == 0, right_edge = sx + 1 >= SX;
+    const uint32_t send_mask = (left_edge ? ~1u : ~0u) & (right_edge ? 0x7FFFFFFFu : ~0u);
+    const int lane_l = (int)((tid + 31u) & 31u), lane_r = (int)((tid + 1u) & 31u);
     const int zs = in_seg ? (int)(seg * P.seg_len) : (int)Z;
     const int ze = min(zs + (int)P.seg_len, (int)Z);
     const int L = max(ze - zs, 0);
@@ -113,12 +119,9 @@ __global__ void __launch_bounds__(1024) k_resident(ResLaunch P, const ResSim* __
             return (has && z >= 0 && z < (int)Z) ? my_g[(size_t)z * plane] : make_uint4(0, 0, 0, 0);
         };
         auto row_of = [&](uint4 st) -> Row {
-            const uint32_t a = alive_plane(st, R);
-            uint32_t al = __shfl_up_sync(0xFFFFFFFFu, a, 1, SXp);
-            uint32_t ar = __shfl_down_sync(0xFFFFFFFFu, a, 1, SXp);
-            al = left_edge ? 0u : al;
-            ar = right_edge ? 0u : ar;
-            return make_row(a, al, ar);
+            const uint32_t a = alive_plane(st, R);  // zero for absent strips
+            const uint32_t v = a & send_mask;
+            return make_row(a, __shfl_sync(0xFFFFFFFFu, v, lane_l), __shfl_sync(0xFFFFFFFFu, v, lane_r));
         };
 
         cave_grid_info info{0, 0, 0, 0, 0, 0};
@@ -134,7 +137,7 @@ __global__ void __launch_bounds__(1024) k_resident(ResLaunch P, const ResSim* __
             const uint4 s_top = L > 0 ? load(ze) : make_uint4(0, 0, 0, 0);
             __syncthreads();
             TickAcc acc;
-            acc.reset();
+            acc.reset(P.nseg != 0u ? 1u : 0u);  // nseg >= 1: a 1 the compiler cannot fold (see mad_add)
             uint32_t xbits = 0u;
             for (int k = 0; k < (int)P.seg_len; k++) {
                 const bool act = k < L;

@@ -200,6 +200,12 @@ cave_status cave_prepare_rule(cave_ctx* ctx, const cave_sim_params* params, cons
  * the compiler's output. Returns CAVE_OK, CAVE_ERR_INVALID_ARG or CAVE_ERR_INTERNAL. */
 cave_status cave_jit_compile(const cave_sim_params* params, const uint64_t* validBitmasks, uint32_t nValid,
                              uint32_t maxRuleBits, char* log, size_t log_size);
+/* Starts compiling the specialised kernel for a rule in the background and returns at once (no
+ * device needed; a no-op when CAVE_JIT=off). Later runs with the rule use it once it is ready;
+ * a process may exit while the compile runs (the library waits for it at exit). Returns
+ * CAVE_OK or CAVE_ERR_INVALID_ARG. */
+cave_status cave_jit_compile_async(const cave_sim_params* params, const uint64_t* validBitmasks, uint32_t nValid,
+                                   uint32_t maxRuleBits);
 /* Diagnostics: rule-specialised kernels loaded into this process so far, and tick launches
  * made with them. Either pointer may be NULL. */
 void cave_jit_stats(uint32_t* loaded, uint64_t* launches);

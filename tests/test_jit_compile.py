@@ -91,3 +91,17 @@ def test_in_process_cache_is_immediate(cache_dir):
     t = time.time()
     ok2, _ = cb.jit_compile(p)
     assert ok and ok2 and time.time() - t < 0.05
+
+
+@pytest.mark.parametrize("wait_s", [0.0, 0.3])
+def test_exit_while_compiling(tmp_path, wait_s):
+    """A process may exit while a background compile runs: the library joins the compile thread
+    before NVRTC's own exit-time teardown, so the process still exits cleanly."""
+    code = ("import time, cave_b200 as cb, oracle as O\n"
+            "p = cb.SimParams(*[int(v) for v in O.make_params(14, 0x7, 0x3C, 0x1E0)])\n"
+            f"cb.jit_compile_async(p); time.sleep({wait_s})\n")
+    env = dict(os.environ, CAVE_JIT_CACHE=str(tmp_path))
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stdout + out.stderr
+    # the compile ran to completion before the exit: its cubin is in the cache
+    assert any(f.endswith(".cubin") for f in os.listdir(tmp_path))
