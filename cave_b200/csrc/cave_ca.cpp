@@ -418,6 +418,61 @@ cave_status cave_ctx_last_timing(const cave_ctx* ctx, cave_timing* out) {
 
 }  // extern "C"
 
+// Rows per CTA for cave_run's tick launches. The default (512 threads' worth of rows) is usually
+// best, but the last row tile of a grid can waste most of its CTA (256^3: 5 tiles of 62 rows for
+// 256), and no closed rule picked the fastest shape for every size measured. So the first long
+// run of a grid shape times a few candidates -- the default and the seven with the least total
+// row work (tiles x rows per tile) at up to 576 threads, the most that keeps two CTAs per SM --
+// for five ticks each and keeps the fastest per context (the default unless another is more than
+// 2% faster: short trials are noisy). The trial ticks read the run's input
+// copy and write the other one, which tick 0 overwrites, and add to the first tick's statistics
+// slot, which is cleared afterwards; results do not depend on the tile shape.
+constexpr uint32_t kTuneMinTicks = 100;
+
+static std::vector<uint32_t> row_candidates(uint32_t X, uint32_t Y, uint32_t rows0) {
+    const uint32_t SX = (X + 31u) / 32u;
+    uint32_t SXp = 1;
+    while (SXp < SX) SXp <<= 1;
+    const uint32_t step = std::max(1u, 32u / SXp);
+    const uint32_t hi = std::min(576u / SXp, Y + 2u);
+    std::vector<std::pair<uint64_t, uint32_t>> scored;
+    for (uint32_t r = std::max(3u * step, (rows0 / 2 + step - 1) / step * step); r <= hi; r += step) {
+        if (r == rows0 || r < 3) continue;
+        const uint64_t tiles = (Y + (r - 2) - 1) / (r - 2);
+        scored.push_back({tiles * r, r});
+    }
+    std::sort(scored.begin(), scored.end());
+    std::vector<uint32_t> out{rows0};
+    for (size_t i = 0; i < scored.size() && out.size() < 8; i++) out.push_back(scored[i].second);
+    return out;
+}
+
+// Times one candidate tile: one untimed tick then five timed ones (tick index 0 each time).
+static cudaError_t time_rows(cave_ctx* ctx, cave_grid* g, const DeviceRule& rule, const JitKernels& jk, uint32_t rows,
+                             uint32_t cps, StreamItem* ditems, uint32_t items_cap, cudaEvent_t e0, cudaEvent_t e1,
+                             float* ms) {
+    StreamPlan plan;
+    if (!plan_stream(0, g->X, g->Y, g->Z, (uint32_t)ctx->sm_count * cps, rows, plan) || plan.items.size() > items_cap) {
+        *ms = 1e30f;
+        return cudaSuccess;
+    }
+    cudaError_t e = cudaMemcpyAsync(ditems, plan.items.data(), sizeof(StreamItem) * plan.items.size(),
+                                    cudaMemcpyHostToDevice, ctx->stream);
+    for (int i = 0; i < 6 && e == cudaSuccess; i++) {
+        if (i == 1) e = cudaEventRecord(e0, ctx->stream);
+        if (e != cudaSuccess) break;
+        e = jk ? launch_stream_tick_jit(jk.pick(true, plan.SX == plan.SXp), ditems, (uint32_t)plan.items.size(),
+                                        g->sim, g->strips, plan.SX, plan.SXp, plan.threads, ctx->stream, i > 0, 0)
+               : launch_stream_tick((int)(rule.flags & 7u), (int)rule.nterms, &rule, ditems,
+                                    (uint32_t)plan.items.size(), g->sim, g->strips, plan.SX, plan.SXp, plan.threads,
+                                    ctx->stream, i > 0, 0);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(e1, ctx->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(ms, e0, e1);
+    return e;
+}
+
 static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* host_out, const cave_sim_params* params,
                             const uint64_t* validBitmasks, uint32_t nValid, uint32_t maxRuleBits, uint32_t nticks,
                             uint32_t maxTicks, cave_tick_stats* per_tick, cave_grid_info* info) {
@@ -462,13 +517,12 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
     TickTotals* dtt = nullptr;  // per-tick totals: the statistics are folded after the last tick
     if (per_tick && nticks) CAVE_CUDA(ctx, cudaMalloc(&dticks, sizeof(cave_tick_stats) * nticks));
     s.per_tick = dticks;
-    cudaError_t e = cudaMalloc(&ditems, sizeof(StreamItem) * plan.items.size());
+    // room for the items of any tile shape tried below (their count is at most one per SM x 4)
+    const uint32_t items_cap = std::max<uint32_t>((uint32_t)plan.items.size(), (uint32_t)ctx->sm_count * cps * 4u);
+    cudaError_t e = cudaMalloc(&ditems, sizeof(StreamItem) * items_cap);
     if (e == cudaSuccess && nticks) e = cudaMalloc(&dtt, sizeof(TickTotals) * nticks);
     if (e == cudaSuccess && nticks) e = cudaMemsetAsync(dtt, 0, sizeof(TickTotals) * nticks, ctx->stream);
     s.deferred = dtt;
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(ditems, plan.items.data(), sizeof(StreamItem) * plan.items.size(), cudaMemcpyHostToDevice,
-                            ctx->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(g->sim, &s, sizeof(s), cudaMemcpyHostToDevice, ctx->stream);
     record(ctx, 0);
     if (e == cudaSuccess && host_in)
@@ -481,6 +535,44 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
     // (its first tick counts every statistic; later ticks leave the zero cells to the fold)
     const JitKernels jk = nticks ? jit_stream_kernel(jit_key(s.rule), jm, (uint64_t)g->X * g->Y * g->Z >= kJitMinCells)
                                  : JitKernels{};
+    // tile shape: an override, the context's earlier choice for this shape, or a timing pass
+    if (e == cudaSuccess && !rows_hint && nticks >= kTuneMinTicks && (uint64_t)g->X * g->Y * g->Z >= kJitMinCells) {
+        const TuneKey key{g->X, g->Y, g->Z, (d.flags & 7u) + (jk ? 8u : 0u)};
+        uint32_t rows = 0;
+        {
+            std::lock_guard<std::mutex> lk(ctx->tune_mu);
+            auto it = ctx->run_rows.find(key);
+            if (it != ctx->run_rows.end()) rows = it->second;
+        }
+        if (!rows) {
+            cudaEvent_t e0 = nullptr, e1 = nullptr;
+            e = cudaEventCreate(&e0);
+            if (e == cudaSuccess) e = cudaEventCreate(&e1);
+            float best = 1e30f;
+            for (uint32_t r : row_candidates(g->X, g->Y, plan.rows)) {
+                float ms = 0;
+                if (e == cudaSuccess) e = time_rows(ctx, g, s.rule, jk, r, cps, ditems, items_cap, e0, e1, &ms);
+                if (e == cudaSuccess && r == plan.rows) ms *= 0.98f;  // a challenger must beat the default by 2%
+                if (e == cudaSuccess && ms < best) {
+                    best = ms;
+                    rows = r;
+                }
+            }
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+            if (e == cudaSuccess) e = cudaMemsetAsync(dtt, 0, sizeof(TickTotals), ctx->stream);
+            if (e == cudaSuccess) {
+                std::lock_guard<std::mutex> lk(ctx->tune_mu);
+                ctx->run_rows[key] = rows;
+            }
+        }
+        if (e == cudaSuccess && rows != plan.rows &&
+            !plan_stream(0, g->X, g->Y, g->Z, (uint32_t)ctx->sm_count * cps, rows, plan))
+            return set_error(ctx, CAVE_ERR_INTERNAL, "tile shape chosen by the timing pass could not be planned");
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(ditems, plan.items.data(), sizeof(StreamItem) * plan.items.size(), cudaMemcpyHostToDevice,
+                            ctx->stream);
     for (uint32_t t = 0; t < nticks && e == cudaSuccess; t++)
         e = jk ? launch_stream_tick_jit(jk.pick(t == 0, plan.SX == plan.SXp), ditems, (uint32_t)plan.items.size(), g->sim,
                                         g->strips, plan.SX, plan.SXp, plan.threads, ctx->stream, true, (int)t)

@@ -52,6 +52,9 @@ struct cave_ctx {
     // autotuner results, shared by every batch and server of the context
     std::mutex tune_mu;
     std::map<cave::TuneKey, cave::ExecChoice> tune_cache;
+    // cave_run's tile choice (rows per CTA) per grid shape and tick kernel (key nb: neighbourhood
+    // bits, + 8 for the rule-specialised kernel), found by a short timing pass (cave_ca.cpp)
+    std::map<cave::TuneKey, uint32_t> run_rows;
     // engine staging buffers released by finished engines, reused by the next (freed with the context)
     std::mutex staging_mu;
     std::vector<cave::StagingPair> staging_free;

@@ -162,3 +162,31 @@ def test_device_seeding_matches_reference_hash(ctx, dims, random_fill, density_i
     with cb.Grid(ctx, X, Y, Z) as g:
         g.seed(c, 5)
         assert np.array_equal(g.download(), expect)
+
+
+# ---------------------------------------------------------------- tile shapes
+def test_tile_timing_pass_and_shapes(ctx, monkeypatch):
+    """A long run of a large grid goes through cave_run's tile timing pass (the trial ticks must
+    leave the input and the statistics untouched), and every tile shape gives the same cells and
+    statistics."""
+    G, T = 128, 100  # 2^21 cells and 100 ticks: the smallest run that is tuned
+    thr = O.threshold_from_float(0.40)
+    init = O.seed(G, G, G, random=True, threshold=thr, run_seed=3, max_cell_state=15)
+    params_np = O.make_params(15, 0x7, 0x10, 0x18)
+    cells, expect = init, []
+    for _ in range(T):
+        cells, snap = O.step_fast(G, G, G, params_np, cells)
+        expect.append(tuple(int(v) for v in snap))
+    p = cb.SimParams(*[int(v) for v in params_np])
+    for rows in (None, 8, 12, 20):
+        if rows is None:
+            monkeypatch.delenv("CAVE_STREAM_ROWS", raising=False)
+        else:
+            monkeypatch.setenv("CAVE_STREAM_ROWS", str(rows))
+        with cb.Grid(ctx, G, G, G) as g:
+            g.upload(init)
+            sts, _ = g.run(p, T, 10 ** 6)
+            assert np.array_equal(g.download(), cells), f"rows {rows}: cells differ after {T} ticks"
+        for t in range(T):
+            got = sts[t].as_tuple()
+            assert got[:len(expect[t])] == expect[t], f"rows {rows}: statistics differ at tick {t + 1}"
