@@ -82,14 +82,14 @@ SeedSpec make_seed_spec(uint32_t X, uint32_t Y, uint32_t Z, uint32_t sx, uint32_
 }
 
 bool plan_stream(uint32_t sim_index, uint32_t X, uint32_t Y, uint32_t Z, uint32_t target_ctas, uint32_t rows_hint,
-                 StreamPlan& plan) {
+                 StreamPlan& plan, uint32_t spt) {
     const uint32_t SX = (X + 31u) / 32u;
-    if (SX == 0 || SX > 32 || Y == 0 || Z == 0 || Y > 65535 || Z > 65535) return false;
+    if (SX == 0 || SX > 32 || Y == 0 || Z == 0 || Y > 65535 || Z > 65535 || (spt != 1 && spt != 2)) return false;
     uint32_t SXp = 1;
     while (SXp < SX) SXp <<= 1;
-    const uint32_t step = std::max(1u, 32u / SXp);  // rows must keep threads a multiple of 32
-    uint32_t rows = rows_hint ? rows_hint : std::max(512u / SXp, 3u);
-    rows = std::min(rows, 1024u / SXp);
+    const uint32_t step = std::max(1u, 32u / SXp) * spt;  // rows must keep threads a multiple of 32
+    uint32_t rows = rows_hint ? rows_hint : std::max(512u * spt / SXp, 3u);
+    rows = std::min(rows, 1024u / SXp);  // at most 1024 threads, 512 with two rows per thread
     rows = std::min(rows, Y + 2u);
     rows = (rows + step - 1) / step * step;
     if (rows < 3) rows = 3 * step;
@@ -103,7 +103,7 @@ bool plan_stream(uint32_t sim_index, uint32_t X, uint32_t Y, uint32_t Z, uint32_
     plan.SX = SX;
     plan.SXp = SXp;
     plan.rows = rows;
-    plan.threads = rows * SXp;
+    plan.threads = rows * SXp / spt;
     plan.ny = ny;
     plan.nz = nz;
     plan.items.clear();
@@ -424,17 +424,32 @@ cave_status cave_ctx_last_timing(const cave_ctx* ctx, cave_timing* out) {
 // run of a grid shape times a few candidates -- the default and the seven with the least total
 // row work (tiles x rows per tile) at up to 576 threads, the most that keeps two CTAs per SM --
 // for five ticks each and keeps the fastest per context (the default unless another is more than
-// 2% faster: short trials are noisy). The trial ticks read the run's input
+// 2% faster: short trials are noisy). With the rule-specialised kernels (two rows per thread) the
+// candidates stay at or below 512 threads. The trial ticks read the run's input
 // copy and write the other one, which tick 0 overwrites, and add to the first tick's statistics
 // slot, which is cleared afterwards; results do not depend on the tile shape.
 constexpr uint32_t kTuneMinTicks = 100;
 
-static std::vector<uint32_t> row_candidates(uint32_t X, uint32_t Y, uint32_t rows0) {
+// The plan of one cave_run tile shape: `rows` per CTA (0 = default) at `spt` rows per thread.
+// Generic kernels: `cps` CTAs per SM (default 2). Rule-specialised kernels (two rows per
+// thread, one 512-thread CTA per SM by registers): as many CTAs per SM as 512-thread
+// equivalents, unless `cps` was given.
+static bool run_plan(const cave_ctx* ctx, const cave_grid* g, uint32_t rows, uint32_t spt, uint32_t cps,
+                     bool cps_given, StreamPlan& plan) {
+    const uint32_t sms = (uint32_t)ctx->sm_count;
+    if (spt == 1) return plan_stream(0, g->X, g->Y, g->Z, sms * cps, rows, plan, 1);
+    if (!plan_stream(0, g->X, g->Y, g->Z, sms * (cps_given ? cps : 1u), rows, plan, spt)) return false;
+    if (!cps_given && plan.threads < 512u)
+        return plan_stream(0, g->X, g->Y, g->Z, sms * (512u / plan.threads), plan.rows, plan, spt);
+    return true;
+}
+
+static std::vector<uint32_t> row_candidates(uint32_t X, uint32_t Y, uint32_t rows0, uint32_t spt) {
     const uint32_t SX = (X + 31u) / 32u;
     uint32_t SXp = 1;
     while (SXp < SX) SXp <<= 1;
-    const uint32_t step = std::max(1u, 32u / SXp);
-    const uint32_t hi = std::min(576u / SXp, Y + 2u);
+    const uint32_t step = std::max(1u, 32u / SXp) * spt;
+    const uint32_t hi = std::min((spt == 1 ? 576u : 512u) * spt / SXp, Y + 2u);
     std::vector<std::pair<uint64_t, uint32_t>> scored;
     for (uint32_t r = std::max(3u * step, (rows0 / 2 + step - 1) / step * step); r <= hi; r += step) {
         if (r == rows0 || r < 3) continue;
@@ -447,15 +462,9 @@ static std::vector<uint32_t> row_candidates(uint32_t X, uint32_t Y, uint32_t row
     return out;
 }
 
-// Times one candidate tile: one untimed tick then five timed ones (tick index 0 each time).
-static cudaError_t time_rows(cave_ctx* ctx, cave_grid* g, const DeviceRule& rule, const JitKernels& jk, uint32_t rows,
-                             uint32_t cps, StreamItem* ditems, uint32_t items_cap, cudaEvent_t e0, cudaEvent_t e1,
-                             float* ms) {
-    StreamPlan plan;
-    if (!plan_stream(0, g->X, g->Y, g->Z, (uint32_t)ctx->sm_count * cps, rows, plan) || plan.items.size() > items_cap) {
-        *ms = 1e30f;
-        return cudaSuccess;
-    }
+// Times one candidate plan: one untimed tick then five timed ones (tick index 0 each time).
+static cudaError_t time_plan(cave_ctx* ctx, cave_grid* g, const DeviceRule& rule, const JitKernels& jk,
+                             const StreamPlan& plan, StreamItem* ditems, cudaEvent_t e0, cudaEvent_t e1, float* ms) {
     cudaError_t e = cudaMemcpyAsync(ditems, plan.items.data(), sizeof(StreamItem) * plan.items.size(),
                                     cudaMemcpyHostToDevice, ctx->stream);
     for (int i = 0; i < 6 && e == cudaSuccess; i++) {
@@ -517,10 +526,7 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
     TickTotals* dtt = nullptr;  // per-tick totals: the statistics are folded after the last tick
     if (per_tick && nticks) CAVE_CUDA(ctx, cudaMalloc(&dticks, sizeof(cave_tick_stats) * nticks));
     s.per_tick = dticks;
-    // room for the items of any tile shape tried below (their count is at most one per SM x 4)
-    const uint32_t items_cap = std::max<uint32_t>((uint32_t)plan.items.size(), (uint32_t)ctx->sm_count * cps * 4u);
-    cudaError_t e = cudaMalloc(&ditems, sizeof(StreamItem) * items_cap);
-    if (e == cudaSuccess && nticks) e = cudaMalloc(&dtt, sizeof(TickTotals) * nticks);
+    cudaError_t e = nticks ? cudaMalloc(&dtt, sizeof(TickTotals) * nticks) : cudaSuccess;
     if (e == cudaSuccess && nticks) e = cudaMemsetAsync(dtt, 0, sizeof(TickTotals) * nticks, ctx->stream);
     s.deferred = dtt;
     if (e == cudaSuccess) e = cudaMemcpyAsync(g->sim, &s, sizeof(s), cudaMemcpyHostToDevice, ctx->stream);
@@ -535,7 +541,11 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
     // (its first tick counts every statistic; later ticks leave the zero cells to the fold)
     const JitKernels jk = nticks ? jit_stream_kernel(jit_key(s.rule), jm, (uint64_t)g->X * g->Y * g->Z >= kJitMinCells)
                                  : JitKernels{};
-    // tile shape: an override, the context's earlier choice for this shape, or a timing pass
+    // tile shape: an override, the context's earlier choice for this shape, or a timing pass;
+    // the rule-specialised kernels take two rows per thread
+    const uint32_t spt = jk ? (uint32_t)kJitRowsPerThread : 1u;
+    if (e == cudaSuccess && !run_plan(ctx, g, rows_hint, spt, cps, env_cps != nullptr, plan))
+        return set_error(ctx, CAVE_ERR_INTERNAL, "streaming plan failed");
     if (e == cudaSuccess && !rows_hint && nticks >= kTuneMinTicks && (uint64_t)g->X * g->Y * g->Z >= kJitMinCells) {
         const TuneKey key{g->X, g->Y, g->Z, (d.flags & 7u) + (jk ? 8u : 0u)};
         uint32_t rows = 0;
@@ -545,31 +555,42 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
             if (it != ctx->run_rows.end()) rows = it->second;
         }
         if (!rows) {
+            std::vector<StreamPlan> cands;
+            size_t most = 0;
+            for (uint32_t r : row_candidates(g->X, g->Y, plan.rows, spt)) {
+                StreamPlan c;
+                if (!run_plan(ctx, g, r, spt, cps, env_cps != nullptr, c)) continue;
+                most = std::max(most, c.items.size());
+                cands.push_back(std::move(c));
+            }
             cudaEvent_t e0 = nullptr, e1 = nullptr;
+            StreamItem* titems = nullptr;
             e = cudaEventCreate(&e0);
             if (e == cudaSuccess) e = cudaEventCreate(&e1);
+            if (e == cudaSuccess) e = cudaMalloc(&titems, sizeof(StreamItem) * std::max<size_t>(most, 1));
             float best = 1e30f;
-            for (uint32_t r : row_candidates(g->X, g->Y, plan.rows)) {
+            for (const StreamPlan& c : cands) {
                 float ms = 0;
-                if (e == cudaSuccess) e = time_rows(ctx, g, s.rule, jk, r, cps, ditems, items_cap, e0, e1, &ms);
-                if (e == cudaSuccess && r == plan.rows) ms *= 0.98f;  // a challenger must beat the default by 2%
+                if (e == cudaSuccess) e = time_plan(ctx, g, s.rule, jk, c, titems, e0, e1, &ms);
+                if (e == cudaSuccess && c.rows == plan.rows) ms *= 0.98f;  // a challenger must beat the default by 2%
                 if (e == cudaSuccess && ms < best) {
                     best = ms;
-                    rows = r;
+                    rows = c.rows;
                 }
             }
             if (e0) cudaEventDestroy(e0);
             if (e1) cudaEventDestroy(e1);
+            cudaFree(titems);
             if (e == cudaSuccess) e = cudaMemsetAsync(dtt, 0, sizeof(TickTotals), ctx->stream);
             if (e == cudaSuccess) {
                 std::lock_guard<std::mutex> lk(ctx->tune_mu);
                 ctx->run_rows[key] = rows;
             }
         }
-        if (e == cudaSuccess && rows != plan.rows &&
-            !plan_stream(0, g->X, g->Y, g->Z, (uint32_t)ctx->sm_count * cps, rows, plan))
+        if (e == cudaSuccess && rows != plan.rows && !run_plan(ctx, g, rows, spt, cps, env_cps != nullptr, plan))
             return set_error(ctx, CAVE_ERR_INTERNAL, "tile shape chosen by the timing pass could not be planned");
     }
+    if (e == cudaSuccess) e = cudaMalloc(&ditems, sizeof(StreamItem) * plan.items.size());
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(ditems, plan.items.data(), sizeof(StreamItem) * plan.items.size(), cudaMemcpyHostToDevice,
                             ctx->stream);

@@ -94,9 +94,10 @@ struct StreamPlan {
 };
 // Builds the work items of simulation `sim_index` with grid X*Y*Z; `target_ctas` is the
 // number of CTAs one tick should spread over (a multiple of the SM count); rows_hint = rows
-// per CTA including the two halo rows (0 = default).
+// per CTA including the two halo rows (0 = default); spt = rows per thread (1, or 2 for the
+// rule-specialised kernels): threads = rows * SXp / spt, a whole number of warps.
 bool plan_stream(uint32_t sim_index, uint32_t X, uint32_t Y, uint32_t Z, uint32_t target_ctas,
-                 uint32_t rows_hint, StreamPlan& plan);
+                 uint32_t rows_hint, StreamPlan& plan, uint32_t spt = 1);
 
 SeedSpec make_seed_spec(uint32_t X, uint32_t Y, uint32_t Z, uint32_t sx, uint32_t sy, uint32_t sz,
                         uint32_t spawnSizeIndex, uint64_t threshold, bool fill_all, uint32_t seed,

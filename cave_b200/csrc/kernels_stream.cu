@@ -217,7 +217,7 @@ cudaError_t launch_stream_tick_jit(cudaKernel_t k, const StreamItem* items, uint
                                    bool pdl, int tick_arg) {
     uint32_t lg = 0;
     while ((1u << lg) < SXp) lg++;
-    const size_t smem = stream_smem_bytes(threads / SXp, SX, SXp);
+    const size_t smem = stream_smem_bytes(kJitRowsPerThread * threads / SXp, SX, SXp);
     {
         // the largest dynamic shared memory set so far, per kernel and device
         static std::mutex mu;

@@ -37,10 +37,20 @@ cave_status cave_render_step(cave_ctx* ctx, const uint32_t* d_in, uint32_t* d_ou
     decode_params(*params, nullptr, 0, 0, d);
     const uint32_t pad = (d.flags & 8u) ? 1u : 0u;  // W flag: WRAP_AT_BOUNDARY
     const RenderGeom g = render_geometry(X, Y, Z, pad);
-    StreamPlan plan;
-    if (!plan_stream(0, g.Xp, g.Yp, g.Zp, (uint32_t)ctx->sm_count * 2u, 0, plan))
-        return set_error(ctx, CAVE_ERR_INVALID_ARG, "render grid too large for the streaming kernel (X <= 1022)");
     CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
+    // the rule-specialised kernels when ready (jit.h; two rows per thread, one 512-thread CTA
+    // per SM-equivalent), else the generic one
+    const JitKernels jk = nticks ? jit_stream_kernel(jit_key(make_device_rule(d)), jit_mode(),
+                                                     (uint64_t)X * Y * Z >= kJitMinCells)
+                                 : JitKernels{};
+    StreamPlan plan;
+    bool planned = jk ? plan_stream(0, g.Xp, g.Yp, g.Zp, (uint32_t)ctx->sm_count, 0, plan, kJitRowsPerThread)
+                      : plan_stream(0, g.Xp, g.Yp, g.Zp, (uint32_t)ctx->sm_count * 2u, 0, plan);
+    if (planned && jk && plan.threads < 512u)
+        planned = plan_stream(0, g.Xp, g.Yp, g.Zp, (uint32_t)ctx->sm_count * (512u / plan.threads), plan.rows, plan,
+                              kJitRowsPerThread);
+    if (!planned)
+        return set_error(ctx, CAVE_ERR_INVALID_ARG, "render grid too large for the streaming kernel (X <= 1022)");
     const uint64_t nstrips = (uint64_t)g.SX * g.Yp * g.Zp;
     uint4* strips = nullptr;
     StripSim* rec = nullptr;
@@ -83,10 +93,8 @@ cave_status cave_render_step(cave_ctx* ctx, const uint32_t* d_in, uint32_t* d_ou
         e = cudaMemcpyAsync(items, plan.items.data(), sizeof(StreamItem) * plan.items.size(), cudaMemcpyHostToDevice,
                             ctx->stream);
     if (e == cudaSuccess) e = launch_render_to_strips(d_in, strips, g, ctx->stream);
-    // the rule-specialised kernel when one is ready (jit.h), else the generic one
-    // (its first tick counts every statistic; later ticks leave the zero cells to the fold)
-    const JitKernels jk =
-        nticks ? jit_stream_kernel(jit_key(s.rule), jit_mode(), (uint64_t)X * Y * Z >= kJitMinCells) : JitKernels{};
+    // (the first tick of the specialised kernels counts every statistic; later ticks leave the
+    // zero cells to the fold)
     for (uint32_t t = 0; t < nticks && e == cudaSuccess; t++) {
         if (pad) e = launch_ghost_fill(strips + (uint64_t)(t & 1u) * nstrips, g, ctx->stream);
         const bool pdl = t > 0 && !pad;

@@ -24,6 +24,7 @@ __device__ __forceinline__ uint4 pack_planes(const uint32_t* p) {
 
 constexpr int kXch = 2;       // y-exchange buffers (double-buffered)
 
+
 // Shared-memory layout (dynamic): ring[kRing][rows*SX] uint4, xch[kXch][rows*SXp] uint4, mbarriers.
 __host__ __device__ inline size_t stream_smem_bytes(uint32_t rows, uint32_t SX, uint32_t SXp) {
     return (size_t)kRing * rows * SX * 16 + (size_t)kXch * rows * SXp * 16 + kRing * 8 + 16;

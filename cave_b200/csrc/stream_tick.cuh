@@ -52,7 +52,7 @@ struct RuntimeRule {
 // box of the tick's input into the previous tick's slot, kPopNone leaves them out (the first
 // tick of such a run; a pass over the final grid supplies the last tick's).
 template <int NB, int NT, bool PR, class Fixed, bool kCountZero = true, bool kDense = false,
-          int kPop = kPopOutput>
+          int kPop = kPopOutput, int kStrips = 1>
 __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ items, StripSim* sims, uint4* pool,
                                                  uint32_t sxp_log2, int tick_arg, const DeviceRule& prule) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -61,7 +61,7 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
     const StreamItem it = items[blockIdx.x];
     StripSim* sim = sims + it.sim;
     const uint32_t SXp = 1u << sxp_log2;
-    const uint32_t rows = blockDim.x >> sxp_log2;  // incl. the two halo rows
+    const uint32_t rows = kStrips * (blockDim.x >> sxp_log2);  // incl. the two halo rows
     // A record's geometry, cell buffers and rule stay fixed while its simulation runs, so they
     // are read while the previous tick drains, before griddepcontrol.wait. (A launch that may
     // start early is never the first one after the record was written: those are launched
@@ -109,11 +109,18 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
         reinterpret_cast<const uint4*>(reinterpret_cast<unsigned char*>(pool) + ((tick & 1u) ? buf1 : buf0));
     uint4* dst = reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(pool) + ((tick & 1u) ? buf0 : buf1));
 
-    const uint32_t sx = threadIdx.x & (SXp - 1u), yy = threadIdx.x >> sxp_log2;
-    const int y = (int)it.y0 - 1 + (int)yy;
-    const bool has = sx < SX && y >= 0 && y < (int)Y && yy < (uint32_t)it.ty + 2u;
-    const bool outp = has && yy >= 1 && yy <= it.ty;
-    const uint32_t valid = has ? strip_valid(sx, X) : 0u;
+    const uint32_t sx = threadIdx.x & (SXp - 1u), yy0 = kStrips * (threadIdx.x >> sxp_log2);
+    int y[kStrips];
+    bool has[kStrips], outp[kStrips];
+#pragma unroll
+    for (int q = 0; q < kStrips; q++) {
+        const uint32_t yy = yy0 + q;
+        y[q] = (int)it.y0 - 1 + (int)yy;
+        has[q] = sx < SX && y[q] >= 0 && y[q] < (int)Y && yy < (uint32_t)it.ty + 2u;
+        outp[q] = has[q] && yy >= 1 && yy <= it.ty;
+    }
+    // valid cells of this column's strips (the rows a thread outputs are all present)
+    const uint32_t valid = (kStrips == 1 ? has[0] : sx < SX) ? strip_valid(sx, X) : 0u;
     // x-neighbour bits travel by rotation inside the warp: lane - 1 (mod 32) holds the previous
     // strip of the row or, for a row's first strip, the last lane of the previous row (or of the
     // warp), which is a right edge or an absent strip; symmetrically for lane + 1. Each thread
@@ -155,12 +162,16 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
         for (int f = 0; f < kRing; f++) issue(f);
     }
 
-    const uint4* my_ring = ring + (size_t)yy * SX + sx;
+    const uint4* my_ring = ring + (size_t)yy0 * SX + sx;  // row q at + q * SX
     if constexpr (kDense) {
         // rows the plane copies never write (outside the grid or the tile) read as dead cells
-        if (!has) {
 #pragma unroll
-            for (int s = 0; s < kRing; s++) const_cast<uint4*>(my_ring)[(size_t)s * slot_stride] = make_uint4(0, 0, 0, 0);
+        for (int q = 0; q < kStrips; q++) {
+            if (!has[q]) {
+#pragma unroll
+                for (int s = 0; s < kRing; s++)
+                    const_cast<uint4*>(my_ring)[(size_t)s * slot_stride + (size_t)q * SX] = make_uint4(0, 0, 0, 0);
+            }
         }
     }
     uint32_t err = 0;
@@ -173,65 +184,107 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
     using P = typename ColumnsFor<NB, Fixed::kFixed>::type;  // carry-save Moore columns when specialised
     TickAcc acc;
     acc.reset(SX != 0u ? 1u : 0u);  // SX >= 1: a 1 the compiler cannot fold
-    uint32_t xbits = 0u;
-    uint4* my_x = xch + threadIdx.x;
-    uint4* my_dst = dst + ((size_t)max(y, 0) * SX + sx);
+    uint32_t xbits[kStrips];
+    uint4* my_dst[kStrips];
+#pragma unroll
+    for (int q = 0; q < kStrips; q++) {
+        xbits[q] = 0u;
+        my_dst[q] = dst + ((size_t)max(y[q], 0) * SX + sx);
+    }
+    uint4* my_x = xch + (size_t)yy0 * SXp + sx;  // row q at + q * SXp
     const size_t plane_stride = (size_t)Y * SX;
     const size_t xpar = (size_t)rows * SXp;
 
     int zo = zfirst + zstep;
     // Fetch f is the (f / kRing)-th use of slot f % kRing, so the phase parity to wait for is
     // (f / kRing) & 1.
-    auto read = [&](int f, int s) -> uint4 {  // s == f % kRing
+    auto read = [&](int f, int s, uint4* out) {  // s == f % kRing
         const int p = zfirst + f * zstep;
-        if (f >= nfetch || (unsigned)p >= Z) return make_uint4(0, 0, 0, 0);
+        if (f >= nfetch || (unsigned)p >= Z) {
+#pragma unroll
+            for (int q = 0; q < kStrips; q++) out[q] = make_uint4(0, 0, 0, 0);
+            return;
+        }
         if (!mbar_wait_bounded(&bars[s], (uint32_t)(f >> kRingLog2) & 1u, kWaitLimitNs)) err = kErrWaitTimeout;
-        return has ? my_ring[(size_t)s * slot_stride] : make_uint4(0, 0, 0, 0);
+#pragma unroll
+        for (int q = 0; q < kStrips; q++)
+            out[q] = has[q] ? my_ring[(size_t)s * slot_stride + (size_t)q * SX] : make_uint4(0, 0, 0, 0);
     };
-    Row r_m = row_of(read(0, 0));
-    uint4 s_c = read(1, 1);
-    Row r_c = row_of(s_c);
+    Row r_m[kStrips], r_c[kStrips];
+    uint4 s_c[kStrips];
+    {
+        uint4 t0[kStrips];
+        read(0, 0, t0);
+        read(1, 1, s_c);
+#pragma unroll
+        for (int q = 0; q < kStrips; q++) {
+            r_m[q] = row_of(t0[q]);
+            r_c[q] = row_of(s_c[q]);
+        }
+    }
     __syncthreads();  // slots 0 and 1 consumed
     if (threadIdx.x == producer) {
         fence_proxy_async();
         issue(kRing);
         issue(kRing + 1);
     }
-    // One plane: the next input plane's rows and column sums, the y-exchange, then the output
-    // strip. U: the plane's position in the unrolled group (selects the exchange buffer).
-    // `checked`: the fetch may lie outside the grid -- only the last plane's fetch can (fetch
-    // f <= L reads plane z0 - 1 + f, or z1 - f when marching down, inside [z0, z1)).
     auto body = [&](int k, const int U, const bool checked) {
         const int f = k + 2, s = f & (kRing - 1);
-        uint4 s_in;
+        uint4 s_in[kStrips];
         if (checked) {
-            s_in = read(f, s);
+            read(f, s, s_in);
         } else {
             if (!mbar_wait_bounded(&bars[s], (uint32_t)(f >> kRingLog2) & 1u, kWaitLimitNs)) err = kErrWaitTimeout;
-            s_in = (kDense || has) ? my_ring[(size_t)s * slot_stride] : make_uint4(0, 0, 0, 0);
+#pragma unroll
+            for (int q = 0; q < kStrips; q++)
+                s_in[q] = (kDense || has[q]) ? my_ring[(size_t)s * slot_stride + (size_t)q * SX] : make_uint4(0, 0, 0, 0);
         }
-        const Row r_p = row_of(s_in);
-        uint32_t pc[P::NC], ps[P::NS];
-        P::make(r_m, r_c, r_p, pc, ps);
+        Row r_p[kStrips];
+        uint32_t pc[kStrips][P::NC], ps[kStrips][P::NS];
+#pragma unroll
+        for (int q = 0; q < kStrips; q++) {
+            r_p[q] = row_of(s_in[q]);
+            P::make(r_m[q], r_c[q], r_p[q], pc[q], ps[q]);
+        }
         uint4* xb = my_x + (size_t)(U & 1) * xpar;
-        *xb = pack_planes<P::NS>(ps);
+        xb[0] = pack_planes<P::NS>(ps[0]);
+        if constexpr (kStrips > 1) xb[(size_t)(kStrips - 1) * SXp] = pack_planes<P::NS>(ps[kStrips - 1]);
         __syncthreads();
         if (threadIdx.x == producer) {
             fence_proxy_async();
             issue(f + kRing);
         }
-        if (outp) {
-            const uint4 qm = *(xb - SXp), qp = *(xb + SXp);
-            const uint32_t psm[4] = {qm.x, qm.y, qm.z, qm.w}, psp[4] = {qp.x, qp.y, qp.z, qp.w};
-            uint32_t cnt[count_bits(NB)];
-            P::combine(pc, psm, psp, cnt);
-            my_dst[(size_t)zo * plane_stride] =
-                update_strip<NB, NT, kCountZero, Fixed::kFullRange, kPop>(s_c, r_c.a, cnt, valid, R, acc,
-                                                                            xbits, (uint32_t)zo);
+#pragma unroll
+        for (int q = 0; q < kStrips; q++) {
+            if (outp[q]) {
+                uint32_t psm[4], psp[4];
+                if (q == 0) {
+                    const uint4 t = *(xb - SXp);
+                    psm[0] = t.x; psm[1] = t.y; psm[2] = t.z; psm[3] = t.w;
+                } else {
+#pragma unroll
+                    for (int i = 0; i < P::NS; i++) psm[i] = ps[q - 1][i];
+                }
+                if (q == kStrips - 1) {
+                    const uint4 t = *(xb + (size_t)kStrips * SXp);
+                    psp[0] = t.x; psp[1] = t.y; psp[2] = t.z; psp[3] = t.w;
+                } else {
+#pragma unroll
+                    for (int i = 0; i < P::NS; i++) psp[i] = ps[q + 1][i];
+                }
+                uint32_t cnt[count_bits(NB)];
+                P::combine(pc[q], psm, psp, cnt);
+                my_dst[q][(size_t)zo * plane_stride] =
+                    update_strip<NB, NT, kCountZero, Fixed::kFullRange, kPop>(s_c[q], r_c[q].a, cnt, valid, R, acc,
+                                                                                xbits[q], (uint32_t)zo);
+            }
         }
-        r_m = r_c;
-        r_c = r_p;
-        s_c = s_in;
+#pragma unroll
+        for (int q = 0; q < kStrips; q++) {
+            r_m[q] = r_c[q];
+            r_c[q] = r_p[q];
+            s_c[q] = s_in[q];
+        }
         zo += zstep;
     };
     static_assert(kUnroll == 6, "the march is unrolled six times");
@@ -248,10 +301,19 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
 
     // ---- per-CTA reduction of the tick statistics
     uint32_t bx0 = 0xFFFFFFFFu, bx1 = 0u, by0 = 0xFFFFFFFFu, by1 = 0u;
-    if (xbits) {
-        bx0 = sx * 32u + (uint32_t)(__ffs(xbits) - 1);
-        bx1 = sx * 32u + 31u - (uint32_t)__clz(xbits);
-        by0 = by1 = (uint32_t)y;
+    uint32_t xall = xbits[0];
+    if (xbits[0]) by0 = by1 = (uint32_t)y[0];
+#pragma unroll
+    for (int q = 1; q < kStrips; q++) {  // rows in increasing y
+        xall |= xbits[q];
+        if (xbits[q]) {
+            by0 = min(by0, (uint32_t)y[q]);
+            by1 = (uint32_t)y[q];
+        }
+    }
+    if (xall) {
+        bx0 = sx * 32u + (uint32_t)(__ffs(xall) - 1);
+        bx1 = sx * 32u + 31u - (uint32_t)__clz(xall);
     }
     uint32_t v[11] = {acc.surviving, acc.born, acc.zero, acc.population, bx0, by0, acc.zmin, bx1, by1, acc.zmax, err};
 #pragma unroll
