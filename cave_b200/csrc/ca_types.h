@@ -18,11 +18,15 @@ struct RuleTerm {
 };
 static_assert(sizeof(RuleTerm) == 32, "RuleTerm is two 16-byte words");
 
-// Rows per thread of the rule-specialised tick kernels (launched with at most 512 threads, one
-// CTA per SM: the two rows' registers would not fit two CTAs). Two rows per thread halve the
-// per-plane work that does not depend on the rows (waits, barrier, loop and address arithmetic,
-// exchange reads), and the rows share their exchange: 512^3 tick 34.1 -> 27.5 us.
-constexpr int kJitRowsPerThread = 2;
+// Rows per thread of the rule-specialised tick kernels (one CTA per SM: the rows' registers
+// would not fit two). Several rows per thread share the per-plane work that does not depend on
+// the rows (waits, barrier, loop and address arithmetic) and keep the pair's inner y-neighbours
+// in registers: 512^3 tick 34.1 us at one row, 27.7 at two, 27.6 at three (256^3: 7.2 -> 6.9).
+constexpr int kJitRowsPerThread = 3;
+// Most threads per CTA of those kernels (their __launch_bounds__): the registers of
+// kJitRowsPerThread rows (three: about 155) and the ring of rows x strips in shared memory must
+// fit one CTA per SM.
+constexpr int kJitMaxThreads = kJitRowsPerThread == 2 ? 512 : 384;
 
 constexpr int kMaxTerms = 8;        // capacity of DeviceRule::terms
 constexpr int kMaxSparseTerms = 4;  // the kernels' sparse evaluation handles up to this many terms

@@ -84,12 +84,13 @@ SeedSpec make_seed_spec(uint32_t X, uint32_t Y, uint32_t Z, uint32_t sx, uint32_
 bool plan_stream(uint32_t sim_index, uint32_t X, uint32_t Y, uint32_t Z, uint32_t target_ctas, uint32_t rows_hint,
                  StreamPlan& plan, uint32_t spt) {
     const uint32_t SX = (X + 31u) / 32u;
-    if (SX == 0 || SX > 32 || Y == 0 || Z == 0 || Y > 65535 || Z > 65535 || (spt != 1 && spt != 2)) return false;
+    if (SX == 0 || SX > 32 || Y == 0 || Z == 0 || Y > 65535 || Z > 65535 || spt < 1 || spt > 3) return false;
     uint32_t SXp = 1;
     while (SXp < SX) SXp <<= 1;
     const uint32_t step = std::max(1u, 32u / SXp) * spt;  // rows must keep threads a multiple of 32
-    uint32_t rows = rows_hint ? rows_hint : std::max(512u * spt / SXp, 3u);
-    rows = std::min(rows, 1024u / SXp);  // at most 1024 threads, 512 with two rows per thread
+    const uint32_t most_threads = spt == 1 ? 1024u : (uint32_t)kJitMaxThreads;
+    uint32_t rows = rows_hint ? rows_hint : std::max((spt == 1 ? 512u : most_threads) * spt / SXp, 3u);
+    rows = std::min(rows, most_threads * spt / SXp);
     rows = std::min(rows, Y + 2u);
     rows = (rows + step - 1) / step * step;
     if (rows < 3) rows = 3 * step;
@@ -424,23 +425,23 @@ cave_status cave_ctx_last_timing(const cave_ctx* ctx, cave_timing* out) {
 // run of a grid shape times a few candidates -- the default and the seven with the least total
 // row work (tiles x rows per tile) at up to 576 threads, the most that keeps two CTAs per SM --
 // for five ticks each and keeps the fastest per context (the default unless another is more than
-// 2% faster: short trials are noisy). With the rule-specialised kernels (two rows per thread) the
-// candidates stay at or below 512 threads. The trial ticks read the run's input
+// 2% faster: short trials are noisy). With the rule-specialised kernels (kJitRowsPerThread rows
+// per thread) the candidates stay at or below kJitMaxThreads threads. The trial ticks read the run's input
 // copy and write the other one, which tick 0 overwrites, and add to the first tick's statistics
 // slot, which is cleared afterwards; results do not depend on the tile shape.
 constexpr uint32_t kTuneMinTicks = 100;
 
 // The plan of one cave_run tile shape: `rows` per CTA (0 = default) at `spt` rows per thread.
-// Generic kernels: `cps` CTAs per SM (default 2). Rule-specialised kernels (two rows per
-// thread, one 512-thread CTA per SM by registers): as many CTAs per SM as 512-thread
-// equivalents, unless `cps` was given.
+// Generic kernels: `cps` CTAs per SM (default 2). Rule-specialised kernels (kJitRowsPerThread
+// rows per thread, one CTA of up to kJitMaxThreads per SM by registers): as many CTAs per SM as
+// kJitMaxThreads-thread equivalents, unless `cps` was given.
 static bool run_plan(const cave_ctx* ctx, const cave_grid* g, uint32_t rows, uint32_t spt, uint32_t cps,
                      bool cps_given, StreamPlan& plan) {
     const uint32_t sms = (uint32_t)ctx->sm_count;
     if (spt == 1) return plan_stream(0, g->X, g->Y, g->Z, sms * cps, rows, plan, 1);
     if (!plan_stream(0, g->X, g->Y, g->Z, sms * (cps_given ? cps : 1u), rows, plan, spt)) return false;
-    if (!cps_given && plan.threads < 512u)
-        return plan_stream(0, g->X, g->Y, g->Z, sms * (512u / plan.threads), plan.rows, plan, spt);
+    if (!cps_given && plan.threads < (uint32_t)kJitMaxThreads)
+        return plan_stream(0, g->X, g->Y, g->Z, sms * ((uint32_t)kJitMaxThreads / plan.threads), plan.rows, plan, spt);
     return true;
 }
 
@@ -449,7 +450,7 @@ static std::vector<uint32_t> row_candidates(uint32_t X, uint32_t Y, uint32_t row
     uint32_t SXp = 1;
     while (SXp < SX) SXp <<= 1;
     const uint32_t step = std::max(1u, 32u / SXp) * spt;
-    const uint32_t hi = std::min((spt == 1 ? 576u : 512u) * spt / SXp, Y + 2u);
+    const uint32_t hi = std::min((spt == 1 ? 576u : (uint32_t)kJitMaxThreads) * spt / SXp, Y + 2u);
     std::vector<std::pair<uint64_t, uint32_t>> scored;
     for (uint32_t r = std::max(3u * step, (rows0 / 2 + step - 1) / step * step); r <= hi; r += step) {
         if (r == rows0 || r < 3) continue;
@@ -542,7 +543,7 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
     const JitKernels jk = nticks ? jit_stream_kernel(jit_key(s.rule), jm, (uint64_t)g->X * g->Y * g->Z >= kJitMinCells)
                                  : JitKernels{};
     // tile shape: an override, the context's earlier choice for this shape, or a timing pass;
-    // the rule-specialised kernels take two rows per thread
+    // the rule-specialised kernels take kJitRowsPerThread rows per thread
     const uint32_t spt = jk ? (uint32_t)kJitRowsPerThread : 1u;
     if (e == cudaSuccess && !run_plan(ctx, g, rows_hint, spt, cps, env_cps != nullptr, plan))
         return set_error(ctx, CAVE_ERR_INTERNAL, "streaming plan failed");

@@ -57,7 +57,7 @@ struct JitRule {
 };
 }  // namespace cave
 #define CAVE_JIT_KERNEL(NAME, COUNT_ZERO, DENSE)                                                           \
-    extern "C" __global__ void __launch_bounds__(512, 1)                                                   \
+    extern "C" __global__ void __launch_bounds__(cave::kJitMaxThreads, 1)                                  \
         NAME(const cave::StreamItem* __restrict__ items, cave::StripSim* sims, uint4* pool, uint32_t sxp_log2, \
              int tick_arg) {                                                                               \
         cave::stream_tick_body<CAVE_JIT_NB, 0, false, cave::JitRule, COUNT_ZERO, DENSE,                     \

@@ -63,7 +63,7 @@ bool jit_compile(const JitKey& k, std::string* log);
 
 // Launches one tick with a specialised kernel: the arguments of launch_stream_tick without the
 // rule (it is compiled in); the kernels take kJitRowsPerThread rows per thread, so `threads`
-// comes from a plan made with that many rows per thread (at most 512).
+// comes from a plan made with that many rows per thread (at most kJitMaxThreads).
 cudaError_t launch_stream_tick_jit(cudaKernel_t k, const StreamItem* items, uint32_t n_items, StripSim* sims,
                                    uint4* pool, uint32_t SX, uint32_t SXp, uint32_t threads, cudaStream_t st,
                                    bool pdl, int tick_arg);

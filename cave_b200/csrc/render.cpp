@@ -38,7 +38,7 @@ cave_status cave_render_step(cave_ctx* ctx, const uint32_t* d_in, uint32_t* d_ou
     const uint32_t pad = (d.flags & 8u) ? 1u : 0u;  // W flag: WRAP_AT_BOUNDARY
     const RenderGeom g = render_geometry(X, Y, Z, pad);
     CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
-    // the rule-specialised kernels when ready (jit.h; two rows per thread, one 512-thread CTA
+    // the rule-specialised kernels when ready (jit.h; kJitRowsPerThread rows per thread, one CTA
     // per SM-equivalent), else the generic one
     const JitKernels jk = nticks ? jit_stream_kernel(jit_key(make_device_rule(d)), jit_mode(),
                                                      (uint64_t)X * Y * Z >= kJitMinCells)
@@ -46,9 +46,9 @@ cave_status cave_render_step(cave_ctx* ctx, const uint32_t* d_in, uint32_t* d_ou
     StreamPlan plan;
     bool planned = jk ? plan_stream(0, g.Xp, g.Yp, g.Zp, (uint32_t)ctx->sm_count, 0, plan, kJitRowsPerThread)
                       : plan_stream(0, g.Xp, g.Yp, g.Zp, (uint32_t)ctx->sm_count * 2u, 0, plan);
-    if (planned && jk && plan.threads < 512u)
-        planned = plan_stream(0, g.Xp, g.Yp, g.Zp, (uint32_t)ctx->sm_count * (512u / plan.threads), plan.rows, plan,
-                              kJitRowsPerThread);
+    if (planned && jk && plan.threads < (uint32_t)kJitMaxThreads)
+        planned = plan_stream(0, g.Xp, g.Yp, g.Zp, (uint32_t)ctx->sm_count * ((uint32_t)kJitMaxThreads / plan.threads),
+                              plan.rows, plan, kJitRowsPerThread);
     if (!planned)
         return set_error(ctx, CAVE_ERR_INVALID_ARG, "render grid too large for the streaming kernel (X <= 1022)");
     const uint64_t nstrips = (uint64_t)g.SX * g.Yp * g.Zp;
