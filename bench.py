@@ -54,6 +54,8 @@ def parse_args():
     ap.add_argument("--rate", type=float, default=200.0, help="serve: mean request arrivals per second")
     ap.add_argument("--requests", type=int, default=64, help="serve: requests in the timed window")
     ap.add_argument("--sims", type=int, default=2048, help="uneven2048: simulations in the batch")
+    ap.add_argument("--stride", type=int, default=1,
+                    help="sweep49: run every n-th simulation of the sweep (small profiling runs)")
     ap.add_argument("--no-autotune", action="store_true")
     return ap.parse_args()
 
@@ -119,18 +121,23 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def committed_traffic(kernel_key):
-    """DRAM bytes per launch from the committed ncu summary (profiles/<kernel_key>.md)."""
+def committed_profile_value(kernel_key, name):
+    """A `name: value` line of the committed ncu summary profiles/<kernel_key>.md (or None)."""
     p = os.path.join(ROOT, "profiles", f"{kernel_key}.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.startswith("traffic_bytes_per_launch:"):
+        if line.startswith(name + ":"):
             try:
                 return float(line.split(":", 1)[1].strip())
             except ValueError:
                 return None
     return None
+
+
+def committed_traffic(kernel_key):
+    """DRAM bytes per launch from the committed ncu summary (profiles/<kernel_key>.md)."""
+    return committed_profile_value(kernel_key, "traffic_bytes_per_launch")
 
 
 def dist_setup(args):
@@ -359,6 +366,8 @@ def sweep_workload(args, world, rank, local, pg):
         return b
 
     full = sweep_descs(G, seeds, cs_values, rank, world)
+    if args.stride > 1:
+        full = np.ascontiguousarray(full[::args.stride])
     warm = np.ascontiguousarray(full[::32])
     for _ in range(args.warmup):
         with make_batch() as b:
@@ -408,7 +417,9 @@ def sweep_workload(args, world, rank, local, pg):
         "vs_baseline": None, "dtype": "u4 (packed nibble states, bit-sliced integer logic)",
         "data": "synthetic: reference cell hash, 30% fill of a centred 16^3 box, seeds 0..31",
         "config": {"workload": f"49^3 FE sweep: 171 x 171 rules (<= 2 bits) x C in {{2,3,4,5}} x 32 seeds, "
-                               f"{T} ticks with early stop", "simulations": int(n_all),
+                               f"{T} ticks with early stop"
+                               + (f", every {args.stride}th simulation" if args.stride > 1 else ""),
+                   "simulations": int(n_all),
                    "parallelism": f"shards x{world}" if world > 1 else "single GPU",
                    "l2": "grids resident in shared memory; initial grids read once per simulation"},
         "cell_updates_per_s": ticks * G ** 3 * world / (kern / 1e3),
@@ -419,6 +430,11 @@ def sweep_workload(args, world, rank, local, pg):
                 "d2h_bytes_per_step": int(full.size * cb.SIM_RESULT_DTYPE.itemsize)},
         "gpu_launches": int(sum_over_ranks(pg, local, launches)),
         "clocks": clocks,
+        # grids stay in shared memory, so the bound is integer issue: utilisation from the
+        # committed ncu capture of this workload (not measured live)
+        "int_issue": {"issue_active_frac": committed_profile_value("resident_sweep49", "issue_active_frac"),
+                      "alu_pipe_frac": committed_profile_value("resident_sweep49", "alu_pipe_frac"),
+                      "source": "ncu --set full, profiles/resident_sweep49.md"},
     }
     ctx.close()
     return line
