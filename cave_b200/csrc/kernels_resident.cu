@@ -139,14 +139,15 @@ __global__ void __launch_bounds__(1024) k_resident(ResLaunch P, const ResSim* __
             TickAcc acc;
             acc.reset(P.nseg != 0u ? 1u : 0u);  // nseg >= 1: a 1 the compiler cannot fold (see mad_add)
             uint32_t xbits = 0u;
-            for (int k = 0; k < (int)P.seg_len; k++) {
+            // one plane; U = k & 1 (the exchange buffer half) is a constant of each call
+            auto step = [&](int k, const int U) {
                 const bool act = k < L;
                 const int z = zs + k;
                 const uint4 s_in = !act ? make_uint4(0, 0, 0, 0) : (z + 1 < ze ? load(z + 1) : s_top);
                 const Row r_p = row_of(s_in);
                 uint32_t pc[PS::NC], ps[PS::NS];
                 PS::make(r_m, r_c, r_p, pc, ps);
-                uint4* xb = my_x + (size_t)(k & 1) * xpar;
+                uint4* xb = my_x + (size_t)U * xpar;
                 if (in_seg) *xb = to_u4<PS::NS>(ps);
                 __syncthreads();
                 if (act && has) {
@@ -159,7 +160,14 @@ __global__ void __launch_bounds__(1024) k_resident(ResLaunch P, const ResSim* __
                 r_m = r_c;
                 r_c = r_p;
                 s_c = s_in;
+            };
+            const int seg_len = (int)P.seg_len;  // the same for every thread: the barriers match
+            int k = 0;
+            for (; k + 1 < seg_len; k += 2) {
+                step(k, 0);
+                step(k + 1, 1);
             }
+            if (k < seg_len) step(k, 0);
             // ---- tick statistics
             uint32_t bx0 = 0xFFFFFFFFu, bx1 = 0u, by0 = 0xFFFFFFFFu, by1 = 0u;
             if (xbits) {
@@ -185,15 +193,25 @@ __global__ void __launch_bounds__(1024) k_resident(ResLaunch P, const ResSim* __
                 for (int q = 0; q < 11; q++) red[warp][q] = v[q];
             }
             __syncthreads();
-            if (tid == 0) {
+            if (warp == 0) {
+                // lane w takes warp w's values; then a shuffle reduction over the lanes
                 const uint32_t nw = (blockDim.x + 31) >> 5;
-                for (uint32_t w = 1; w < nw; w++) {
-                    for (int q = 0; q < 4; q++) red[0][q] += red[w][q];
-                    for (int q = 4; q < 7; q++) red[0][q] = min(red[0][q], red[w][q]);
-                    for (int q = 7; q < 10; q++) red[0][q] = max(red[0][q], red[w][q]);
-                    red[0][10] |= red[w][10];
+                const bool live = lane < nw;
+#pragma unroll
+                for (int q = 0; q < 11; q++) v[q] = live ? red[lane][q] : ((q >= 4 && q < 7) ? 0xFFFFFFFFu : 0u);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+                    for (int q = 0; q < 4; q++) v[q] += __shfl_xor_sync(0xFFFFFFFFu, v[q], o);
+#pragma unroll
+                    for (int q = 4; q < 7; q++) v[q] = min(v[q], __shfl_xor_sync(0xFFFFFFFFu, v[q], o));
+#pragma unroll
+                    for (int q = 7; q < 10; q++) v[q] = max(v[q], __shfl_xor_sync(0xFFFFFFFFu, v[q], o));
+                    v[10] |= __shfl_xor_sync(0xFFFFFFFFu, v[10], o);
                 }
-                const uint32_t surv = red[0][0], born = red[0][1], zero = red[0][2], pop = red[0][3];
+            }
+            if (tid == 0) {
+                const uint32_t surv = v[0], born = v[1], zero = v[2], pop = v[3];
                 const uint32_t dead = zero - born;
                 const uint32_t dying = volume - dead - born - surv;
                 // searchManager.slang:115-139
@@ -213,10 +231,10 @@ __global__ void __launch_bounds__(1024) k_resident(ResLaunch P, const ResSim* __
                 if (changed) active_ticks++;
                 last_pop = pop;
                 for (int q = 0; q < 3; q++) {
-                    bmin[q] = red[0][4 + q];
-                    bmax[q] = red[0][7 + q];
+                    bmin[q] = v[4 + q];
+                    bmax[q] = v[7 + q];
                 }
-                if (red[0][10]) err |= red[0][10];
+                if (v[10]) err |= v[10];
                 s_stop = info.status != 0;
             }
             __syncthreads();
