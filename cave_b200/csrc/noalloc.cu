@@ -35,51 +35,9 @@ unsigned char* g_scratch_base[kMaxDevices] = {};
 
 constexpr uint64_t align256(uint64_t v) { return (v + 255u) & ~uint64_t(255u); }
 
-// Tiling of one grid for k_stream_tick with the default shape cave_run uses (rows per CTA
-// 512 / SXp, 2 CTAs per SM), computed without building a host item list.
-struct Tiling {
-    uint32_t SX, SXp, rows, threads, ny, ty, nz, slab;
-};
-
-bool tiling(uint32_t X, uint32_t Y, uint32_t Z, uint32_t target_ctas, Tiling& t) {
-    t.SX = (X + 31u) / 32u;
-    if (t.SX == 0 || t.SX > 32 || Y == 0 || Z == 0 || Y > 65535 || Z > 65535) return false;
-    t.SXp = 1;
-    while (t.SXp < t.SX) t.SXp <<= 1;
-    const uint32_t step = std::max(1u, 32u / t.SXp);  // threads stay a multiple of 32
-    uint32_t rows = std::max(512u / t.SXp, 3u);
-    rows = std::min(rows, 1024u / t.SXp);
-    rows = std::min(rows, Y + 2u);
-    rows = (rows + step - 1) / step * step;
-    if (rows < 3) rows = 3 * step;
-    t.rows = rows;
-    t.threads = rows * t.SXp;
-    const uint32_t TY = rows - 2;
-    t.ny = (Y + TY - 1) / TY;
-    t.ty = (Y + t.ny - 1) / t.ny;
-    uint32_t nz = std::max(1u, target_ctas / t.ny);
-    nz = std::min(nz, Z);
-    t.slab = (Z + nz - 1) / nz;
-    t.nz = (Z + t.slab - 1) / t.slab;
-    return true;
-}
-
-// Writes the simulation record and the tick kernel's work items into the scratch array.
-// Every field of the record is rewritten, so nothing from an earlier call survives in it.
-__global__ void k_noalloc_setup(StripSim rec, StripSim* dst, StreamItem* items, uint32_t ny, uint32_t nz,
-                                uint32_t ty, uint32_t slab, uint32_t Y, uint32_t Z) {
-    const uint32_t n = ny * nz;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t iz = i / ny, iy = i - iz * ny;
-        StreamItem it;
-        it.sim = 0;
-        it.y0 = (uint16_t)(iy * ty);
-        it.ty = (uint16_t)min(ty, Y - iy * ty);
-        it.z0 = (uint16_t)(iz * slab);
-        it.z1 = (uint16_t)min(Z, (iz + 1) * slab);
-        it.dir_items = (n << 1) | (iz & 1u);
-        items[i] = it;
-    }
+// Writes the simulation record into the scratch array. Every field is rewritten, so nothing
+// from an earlier call survives in it.
+__global__ void k_noalloc_setup(StripSim rec, StripSim* dst) {
     if (blockIdx.x == 0 && threadIdx.x == 0) *dst = rec;
 }
 
@@ -90,7 +48,17 @@ cave_status scratch_base(cave_ctx* ctx, unsigned char** out) {
     std::lock_guard<std::mutex> lock(g_setup_mu);
     if (!g_scratch_base[ctx->device]) {
         void* p = nullptr;
+        // With lazy module loading (the CUDA default) this is where the module holding the array
+        // is loaded on this device, so this is where its memory is taken.
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);  // ctx's device is current
+        if (e == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            return set_error(ctx, CAVE_ERR_OUT_OF_MEMORY,
+                             "cave_run_noalloc: the device could not hold the static scratch array "
+                             "g_noalloc_scratch (" + std::to_string((uint64_t)kScratchBytes) +
+                                 " bytes); make the first call on a device before another allocator "
+                                 "reserves its memory");
+        }
         if (e != cudaSuccess) return check_cuda(ctx, e, "cudaGetSymbolAddress(scratch)");
         if (!p) return set_error(ctx, CAVE_ERR_CUDA, "cave_run_noalloc: scratch array has no device address");
         g_scratch_base[ctx->device] = static_cast<unsigned char*>(p);
@@ -99,13 +67,16 @@ cave_status scratch_base(cave_ctx* ctx, unsigned char** out) {
     return CAVE_OK;
 }
 
-bool is_device_pointer(const void* p) {
+// Device memory of `device` itself, or managed memory (reachable from every device). Memory of
+// another GPU is rejected: without peer access the kernels would fault on it.
+bool is_device_pointer(const void* p, int device) {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    if (a.type == cudaMemoryTypeManaged) return true;
+    return a.type == cudaMemoryTypeDevice && a.device == device;
 }
 
 }  // namespace
@@ -122,12 +93,14 @@ extern "C" cave_status cave_run_noalloc(cave_ctx* ctx, const uint32_t* d_in, uin
     DecodedRule d;
     if (!decode_params(*params, validBitmasks, nValid, maxRuleBits, d))
         return set_error(ctx, CAVE_ERR_INVALID_ARG, "rule index outside the valid-bitmask table");
-    Tiling t;
-    if (!tiling(X, Y, Z, (uint32_t)ctx->sm_count * 2u, t))
+    // the tile shape cave_run uses by default with the library's tick kernel (two CTAs per SM);
+    // plan_stream builds the work items in host memory only
+    StreamPlan plan;
+    if (!plan_stream(0, X, Y, Z, (uint32_t)ctx->sm_count * 2u, 0, plan, 1))
         return set_error(ctx, CAVE_ERR_INVALID_ARG,
                          "grid shape not supported by the streaming kernel (X <= 1024, Y, Z <= 65535)");
-    const uint64_t nstrips = (uint64_t)t.SX * Y * Z;
-    const uint64_t n_items = (uint64_t)t.ny * t.nz;
+    const uint64_t nstrips = (uint64_t)plan.SX * Y * Z;
+    const uint64_t n_items = plan.items.size();
     const uint64_t items_off = align256(sizeof(StripSim));
     const uint64_t strips_off = align256(items_off + n_items * sizeof(StreamItem));
     const uint64_t need = strips_off + 2 * nstrips * 16;
@@ -141,8 +114,10 @@ extern "C" cave_status cave_run_noalloc(cave_ctx* ctx, const uint32_t* d_in, uin
     if (d_per_tick && (reinterpret_cast<uintptr_t>(d_per_tick) & 7u))
         return set_error(ctx, CAVE_ERR_INVALID_ARG, "cave_run_noalloc: per-tick buffer must be 8-byte aligned");
     CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
-    if (!is_device_pointer(d_in) || !is_device_pointer(d_out) || (d_per_tick && !is_device_pointer(d_per_tick)))
-        return set_error(ctx, CAVE_ERR_INVALID_ARG, "cave_run_noalloc: buffers must be device memory");
+    if (!is_device_pointer(d_in, ctx->device) || !is_device_pointer(d_out, ctx->device) ||
+        (d_per_tick && !is_device_pointer(d_per_tick, ctx->device)))
+        return set_error(ctx, CAVE_ERR_INVALID_ARG,
+                         "cave_run_noalloc: buffers must be device memory of the context's device");
     unsigned char* base = nullptr;
     if (cave_status s = scratch_base(ctx, &base); s != CAVE_OK) return s;
 
@@ -156,7 +131,7 @@ extern "C" cave_status cave_run_noalloc(cave_ctx* ctx, const uint32_t* d_in, uin
     s.X = X;
     s.Y = Y;
     s.Z = Z;
-    s.SX = t.SX;
+    s.SX = plan.SX;
     s.buf[0] = 0;
     s.buf[1] = nstrips * 16;
     s.max_ticks = maxTicks;
@@ -166,13 +141,18 @@ extern "C" cave_status cave_run_noalloc(cave_ctx* ctx, const uint32_t* d_in, uin
     for (int k = 0; k < 3; k++) s.acc_bmin[k] = 0xFFFFFFFFu;
     s.per_tick = nticks ? d_per_tick : nullptr;
 
-    const uint32_t setup_blocks = (uint32_t)std::min<uint64_t>((n_items + 255) / 256, 148);
-    k_noalloc_setup<<<setup_blocks, 256, 0, ctx->stream>>>(s, rec_dev, items, t.ny, t.nz, t.ty, t.slab, Y, Z);
-    cudaError_t e = cudaGetLastError();
+    // the work items travel by a copy from pageable host memory (staged by the driver in host
+    // memory; no device allocation), the record by a one-thread kernel
+    cudaError_t e = cudaMemcpyAsync(items, plan.items.data(), sizeof(StreamItem) * n_items, cudaMemcpyHostToDevice,
+                                    ctx->stream);
+    if (e == cudaSuccess) {
+        k_noalloc_setup<<<1, 32, 0, ctx->stream>>>(s, rec_dev);
+        e = cudaGetLastError();
+    }
     if (e == cudaSuccess) e = launch_nib_to_strips(d_in, pool, X, Y, Z, ctx->stream);
     for (uint32_t k = 0; k < nticks && e == cudaSuccess; k++)
         e = launch_stream_tick((int)(d.flags & 7u), (int)s.rule.nterms, &s.rule, items, (uint32_t)n_items, rec_dev,
-                               pool, t.SX, t.SXp, t.threads, ctx->stream);
+                               pool, plan.SX, plan.SXp, plan.threads, ctx->stream);
     // Raw stepping never stops early, so the result is in copy (nticks & 1).
     if (e == cudaSuccess) e = launch_strips_to_nib(pool + (uint64_t)(nticks & 1u) * nstrips, d_out, X, Y, Z, ctx->stream);
     StripSim back;

@@ -216,18 +216,25 @@ void cave_jit_stats(uint32_t* loaded, uint64_t* launches);
  * allocator, where cudaMalloc can fail, or that cannot take cudaFree's device-wide
  * synchronisation between requests.
  * d_in / d_out: caller-owned DEVICE buffers of cave_grid_words(X, Y, Z) words in the nibble
- * layout (4-byte aligned; d_in == d_out is allowed). d_per_tick: caller-owned device array of
- * nticks entries, or NULL. *info (host, may be NULL) receives the GridInfo as in cave_run.
- * Cells, statistics and GridInfo equal cave_run's for the same inputs. Blocking.
+ * layout (4-byte aligned; d_in == d_out is allowed), in memory of the context's device (or
+ * managed memory); another GPU's memory is rejected with CAVE_ERR_INVALID_ARG. d_per_tick:
+ * caller-owned device array of nticks entries, or NULL. *info (host, may be NULL) receives
+ * the GridInfo as in cave_run. Cells, statistics and GridInfo equal cave_run's for the same
+ * inputs. Blocking. The work runs on the context's own stream, which is not ordered after
+ * any other stream: the caller's writes of d_in must be complete, and d_out not in use, on
+ * every other stream before the call (synchronise those streams, or wait on an event).
  * Scratch: one static device array of CAVE_NOALLOC_SCRATCH_BYTES per GPU, part of the
- * library's device image (held by every GPU that loads the library until exit). A grid needs
- * 32 bytes per 32 x-cells (rounded up) per row and plane plus a few KB; larger grids are
- * rejected with CAVE_ERR_INVALID_ARG (256^3 and 320^3 fit). The first call on a device looks
- * the array up (cudaGetSymbolAddress with that device current); make that first call before
- * any stream capture. Every call on a device shares the array: calls that overlap on the GPU
- * (two contexts, or two host threads, on one device) race and must be serialised by the
- * caller. The simulation record in the array is rewritten by each call. Not timed by
- * cave_ctx_set_timing. */
+ * library's device image. Under CUDA's lazy module loading (the default) a GPU takes that
+ * memory when the first cave_run_noalloc call on it loads the array's module, and then holds
+ * it until exit: make the first call on a device before another allocator reserves that
+ * device's memory (if it cannot be had, the call fails with CAVE_ERR_OUT_OF_MEMORY naming the
+ * array). A grid needs 32 bytes per 32 x-cells (rounded up) per row and plane plus a few KB;
+ * larger grids are rejected with CAVE_ERR_INVALID_ARG (256^3 and 320^3 fit). The first call on
+ * a device looks the array up (cudaGetSymbolAddress with that device current); make that
+ * first call before any stream capture. Every call on a device shares the array: calls that
+ * overlap on the GPU (two contexts, or two host threads, on one device) race and must be
+ * serialised by the caller. The simulation record in the array is rewritten by each call. Not
+ * timed by cave_ctx_set_timing. */
 #define CAVE_NOALLOC_SCRATCH_BYTES (32u << 20)
 cave_status cave_run_noalloc(cave_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t X, uint32_t Y,
                              uint32_t Z, const cave_sim_params* params, const uint64_t* validBitmasks,

@@ -137,3 +137,44 @@ def test_rejects_host_buffers(ctx):
     with pytest.raises(cb.CaveError) as e:
         cb.run_noalloc(ctx, host.ctypes.data, host.ctypes.data, X, Y, Z, cb.make_params(16, 0x7, 16, 24), 1)
     assert "device memory" in str(e.value)
+
+
+def test_call_allocates_no_device_memory(ctx):
+    """A call after the first one on the device leaves the device's free memory unchanged:
+    nothing is allocated or freed on the device. The first call (which loads the scratch array's
+    module and the kernels it uses) has the same rule, so the measured call of another grid shape
+    needs no kernel that is not loaded yet."""
+    torch = _torch()
+    X, Y, Z, init, params, nticks, max_ticks, valid, K = _case_kindex()
+    noalloc_run(ctx, X, Y, Z, init, params, nticks, max_ticks, valid, K)
+    X2, Y2, Z2 = 50, 30, 41
+    init2 = random_cells(np.random.default_rng(9), X2, Y2, Z2, 6)
+    d_in = torch.from_numpy(init2.view(np.int32)).to("cuda:0")
+    d_out = torch.zeros_like(d_in)
+    d_ticks = torch.zeros(nticks * TICK_BYTES, dtype=torch.uint8, device="cuda:0")
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    cb.run_noalloc(ctx, d_in.data_ptr(), d_out.data_ptr(), X2, Y2, Z2, params, nticks, max_ticks, valid, K,
+                   d_ticks.data_ptr())
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0, f"device free memory changed by {free0 - free1} bytes"
+    want = reference_run(ctx, X2, Y2, Z2, init2, params, nticks, max_ticks, valid, K)
+    assert np.array_equal(d_out.cpu().numpy().view(np.uint32), want[0]), "cells differ from cave_run"
+
+
+def test_rejects_memory_of_another_gpu(ctx):
+    """A buffer on another GPU is refused before anything is launched."""
+    torch = _torch()
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs a second GPU")
+    X = Y = Z = 8
+    other = torch.zeros(cb.grid_words(X, Y, Z), dtype=torch.int32, device="cuda:1")
+    mine = torch.zeros_like(other, device="cuda:0")
+    torch.cuda.synchronize(0)
+    torch.cuda.synchronize(1)
+    for a, b in ((other, mine), (mine, other)):
+        with pytest.raises(cb.CaveError) as e:
+            cb.run_noalloc(ctx, a.data_ptr(), b.data_ptr(), X, Y, Z, cb.make_params(16, 0x7, 16, 24), 1)
+        assert e.value.code == 1  # CAVE_ERR_INVALID_ARG
+        assert "context's device" in str(e.value)
