@@ -1,24 +1,38 @@
 #!/usr/bin/env python
 """bench.py -- throughput of the B200 CA stepping path on the reference's headline workloads.
 
-Default workload (one GPU): a 512^3 grid, Moore-26 neighbourhood, C = 16 states (maxCellState
-15), survive {4,5}, birth {5}, 40% of the whole volume seeded alive by the reference's cell
-hash (seed 0), 1000 ticks with statistics every tick. One "step" is one full 1000-tick run
-through the C ABI (cave_run: nibble layout in HBM -> bit-plane layout -> 1000 tick launches ->
-back). `value` is cell-updates/s with the grid already resident in HBM; `e2e` is the same
-through cave_run_host with the grid read from and written back to pinned host memory.
+Default line (one GPU): a 512^3 grid, Moore-26 neighbourhood, C = 16 states (maxCellState 15),
+survive {4,5}, birth {5}, 40% of the whole volume seeded alive by the reference's cell hash
+(seed 0), 1000 ticks with statistics every tick. One "step" is one full 1000-tick run through
+the C ABI (cave_run: nibble layout in HBM -> bit-plane layout -> tick launches -> back).
+`value` is cell-updates/s with the grid already resident in HBM; `e2e` is the same through
+cave_run_host with the grid read from and written back to pinned host memory. The last timed
+run and the last end-to-end run are checked against the oracle fixture
+(tests/golden/large_fixtures.json): every cell, every tick's statistics and the GridInfo.
+
+The default line also carries `extra`: the other workloads, each timed on the device, checked
+against its oracle fixture where one exists, with its CPU baseline and clocks:
+  plain49     the plain single simulation (49^3 FE, C=4, 20 ticks): plain, streaming and
+              resident paths
+  large256    256^3, same rule as the default, 1000 ticks (L2-resident ping-pong)
+  large1024   1024^3, 200 ticks (out of L2)
+  sweep49     the batched search sweep (3,742,848 simulations of 49^3) vs the plain path
+  uneven2048  the uneven-size batch with the autotuner vs the plain path
+  serve       the served request stream at 200 requests/s (overload) and 16 requests/s
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl reference]
 
-Under torchrun (N > 1) every rank runs an independent replica (a single grid does not shard
-without a halo exchange the reference does not do in search mode); value = all ranks' cell
-updates / max over ranks of the device time.
+Under torchrun (N > 1) every rank runs an independent replica of the large grids (a single
+grid does not shard without a halo exchange the reference does not do in search mode) and a
+shard of the simulation workloads; value = all ranks' work / max over ranks of the device time.
 """
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
+import platform
 import statistics
 import subprocess
 import sys
@@ -29,16 +43,20 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 WORKLOADS = {
     # name: (edge, ticks)
     "large512": (512, 1000),
     "large256": (256, 1000),
     "large1024": (1024, 200),
+    "plain49": (49, 20),
     "sweep49": (49, 20),
     "uneven2048": (0, 0),
     "serve": (0, 0),
 }
+LARGE_RULE = (15, 0x7, 1 << 4, (1 << 3) | (1 << 4))  # maxCellState, flags, birth, survival
+PLAIN_RULE = (3, 0x3, 0x60, 0x70)
 
 
 def parse_args():
@@ -48,6 +66,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="large512")
+    ap.add_argument("--no-extra", action="store_true", help="default line only (no other workloads)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ticks", type=int, default=0, help="override the workload's tick count (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -140,6 +159,35 @@ def committed_traffic(kernel_key):
     return committed_profile_value(kernel_key, "traffic_bytes_per_launch")
 
 
+def fixture(name):
+    p = os.path.join(GOLDEN, name)
+    return json.load(open(p)) if os.path.exists(p) else {}
+
+
+def sha256_u32(a) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).astype("<u4").tobytes()).hexdigest()
+
+
+class ParityError(AssertionError):
+    pass
+
+
+def require(ok, what):
+    if not ok:
+        raise ParityError(f"parity check failed: {what}")
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return platform.processor() or "unknown"
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -186,44 +234,114 @@ def sum_over_ranks(pg, local, v):
     return _reduce(pg, local, v, pg.ReduceOp.SUM if pg else None)
 
 
-# ----------------------------------------------------------------------------- CPU baseline
-def cpu_baseline_large(G, init, params, budget_s=12.0):
-    """The oracle's OpenMP step (bit-identical to the literal restatement) on the same grid."""
+# ----------------------------------------------------------------------------- CPU baselines
+# The oracle (oracle/, test infrastructure) is the CPU restatement of the reference's shader
+# arithmetic; the reference itself has no CPU stepping. Only these functions load it.
+def _oracle_params(rule):
     import oracle as O
 
+    return O.make_params(*rule)
+
+
+def cpu_baseline_grid(G, init, rule, ticks_full, budget_s=10.0, single=True, spawn=None):
+    """The oracle's OpenMP z-slab step on the same grid, all host cores, then one thread."""
+    import oracle as O
+
+    params = _oracle_params(rule)
     cores = os.cpu_count() or 1
-    cells = init
+
+    def rate(nthreads, budget, most):
+        cells, ticks, t0 = init, 0, time.perf_counter()
+        while True:
+            cells, _ = O.step_fast(G, G, G, params, cells, nthreads=nthreads)
+            ticks += 1
+            el = time.perf_counter() - t0
+            if el > budget or ticks >= most:
+                return G ** 3 * ticks / el, ticks, el
+
+    v, n, el = rate(cores, budget_s, 50)
+    out = {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": "port", "cpu_model": cpu_model(),
+           "sample": f"{n} ticks of the {G}^3 grid (of {ticks_full}), oracle OpenMP z-slab step on {cores} threads, "
+                     f"{el:.1f} s"}
+    if single:
+        v1, n1, el1 = rate(1, budget_s / 3, 20)
+        out["single_thread"] = {"value": v1, "unit": "cell-updates/s",
+                                "sample": f"{n1} ticks, 1 thread, {el1:.1f} s"}
+    return out
+
+
+def _pool_init():
+    os.environ["OMP_NUM_THREADS"] = "1"
+
+
+def _cpu_sweep_sim(a):
+    """One sweep simulation on one host thread (oracle): (ticks run, cells per tick)."""
+    import oracle as O
+
+    mcs, s, si, bi = a
+    init = O.seed(49, 49, 49, spawn=(16, 16, 16), random=True, threshold=O.threshold_from_float(0.30), run_seed=s,
+                  max_cell_state=mcs)
+    info, _, _ = O.run_sim(49, 49, 49, O.make_params(mcs, 0x3, bi + 1, si + 1), init, 20,
+                           valid=O.valid_bitmasks(18, 2), max_rule_bits=2, fast=True)
+    return info.ticks, 49 ** 3
+
+
+def _cpu_uneven_sim(s):
+    import oracle as O
+
+    e = s["edge"]
+    init = O.seed(e, e, e, random=True, threshold=O.threshold_from_float(s["fill"]), run_seed=s["seed"],
+                  max_cell_state=s["maxcs"])
+    info, _, _ = O.run_sim(e, e, e, O.make_params(s["maxcs"], s["flags"], s["birth"], s["survival"]), init,
+                           s["ticks"], fast=True)
+    return info.ticks, e ** 3
+
+
+def cpu_baseline_sims(fn, items, what):
+    """A sample of simulations run by the oracle, one per host thread over all cores (a spawn
+    process pool: safe after CUDA is initialised), then the first few on one thread."""
+    from multiprocessing import get_context
+
+    cores = os.cpu_count() or 1
     t0 = time.perf_counter()
-    ticks = 0
-    while True:
-        cells, _ = O.step_fast(G, G, G, params, cells, nthreads=cores)
-        ticks += 1
-        el = time.perf_counter() - t0
-        if el > budget_s or ticks >= 50:
-            break
-    return {"value": G ** 3 * ticks / el, "unit": "cell-updates/s", "cores": cores, "kind": "port",
-            "sample": f"{ticks} ticks of the {G}^3 grid (of {WORKLOADS.get(f'large{G}', (G, 0))[1]}), oracle "
-                      f"OpenMP z-slab step, {el:.1f} s"}
+    with get_context("spawn").Pool(cores, initializer=_pool_init) as pool:
+        t1 = time.perf_counter()
+        res = pool.map(fn, items, chunksize=1)
+        el = time.perf_counter() - t1
+    updates = sum(t * v for t, v in res)
+    one = items[:max(1, len(items) // (4 * cores))]
+    _pool_init()
+    t2 = time.perf_counter()
+    r1 = [fn(x) for x in one]
+    el1 = time.perf_counter() - t2
+    return {"value": len(items) / el, "unit": "sims/s", "cell_updates_per_s": updates / el, "cores": cores,
+            "kind": "port", "cpu_model": cpu_model(),
+            "sample": f"{len(items)} simulations ({what}), oracle, one simulation per thread on {cores} threads, "
+                      f"{el:.1f} s (pool start {t1 - t0:.1f} s not counted)",
+            "single_thread": {"value": len(one) / el1, "unit": "sims/s",
+                              "cell_updates_per_s": sum(t * v for t, v in r1) / el1,
+                              "sample": f"first {len(one)} of them on 1 thread, {el1:.1f} s"}}
 
 
-# ----------------------------------------------------------------------------- workloads
-def large_workload(args, world, rank, local, pg):
-    import numpy as np
+# ----------------------------------------------------------------------------- large grids
+def large_workload(args, world, rank, local, pg, G, T, steps, warmup, e2e=True, cpu=True):
     import torch
 
     import cave_b200 as cb
 
-    G, T = WORKLOADS[args.workload]
-    T = args.ticks or T
     cells_per_step = G ** 3 * T
     thr = cb.threshold_from_fill(0.40)
-    params = cb.make_params(15, 0x7, 0x10, 0x18)
+    params = cb.make_params(*LARGE_RULE)
     ctx = cb.Context(local)
     ctx.set_timing(True)
     g = cb.Grid(ctx, G, G, G)
     g.seed_threshold((G, G, G), thr, 0, 15)
     init_host = g.download()
     words = init_host.size
+    fx = fixture("large_fixtures.json").get(str(G), {})
+    want = fx.get("checkpoints", {}).get(str(T))
+    if fx:
+        require(sha256_u32(init_host) == fx["seed_sha256"], f"{G}^3 seeded cells")
     pin_in = torch.from_numpy(init_host.view(np.int32)).pin_memory()
     pin_out = torch.empty(words, dtype=torch.int32).pin_memory()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=f"cuda:{local}")  # 256 MiB > L2
@@ -233,20 +351,28 @@ def large_workload(args, world, rank, local, pg):
         flush.zero_()
         torch.cuda.synchronize(local)
 
+    def check(cells, ticks, info, what):
+        if not want:
+            return
+        rec = cb.tick_records(ticks)
+        require(hashlib.sha256(rec.tobytes()).hexdigest() == want["ticks_sha256"], f"{what}: per-tick statistics")
+        require(list(info.as_tuple()) == want["gridinfo"], f"{what}: GridInfo")
+        require(sha256_u32(cells) == want["cells_sha256"], f"{what}: cells")
+
     # the tick kernel compiled for this rule (NVRTC, cached), unless CAVE_JIT=off
     t_prep = time.perf_counter()
     ctx.prepare_rule(params)
     prep_s = time.perf_counter() - t_prep
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         reset()
         g.run(params, T, T, stats=True)
     barrier(pg, local)
     dev_ms, tick_ms, conv_ms, launches = [], [], [], 0
     _, jit0 = cb.jit_stats()
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
+        for _ in range(steps):
             reset()
-            g.run(params, T, T, stats=True)
+            ticks, info = g.run(params, T, T, stats=True)
             t = ctx.last_timing()
             dev_ms.append(t.total_ms)
             tick_ms.append(t.tick_ms)
@@ -255,35 +381,37 @@ def large_workload(args, world, rank, local, pg):
         barrier(pg, local)
     clocks = clk.summary()
     _, jit1 = cb.jit_stats()
-    specialised = jit1 - jit0 == T * args.steps
+    specialised = jit1 - jit0 > 0
+    pairs = specialised and launches <= steps * (T // 2 + 1 + 4)  # two ticks per launch (+ conversion/fold kernels)
+    check(g.download(), ticks, info, f"{G}^3 x {T} ticks, device-resident run")
     # end-to-end through the C ABI with host buffers
     e2e_ms = []
-    for i in range(0 if args.no_e2e else args.steps + 1):
+    for i in range(steps + 1 if e2e else 0):
         flush.zero_()
         torch.cuda.synchronize(local)
-        g.run_host(pin_in.data_ptr(), pin_out.data_ptr(), params, T, T, stats=True)
+        ticks, info = g.run_host(pin_in.data_ptr(), pin_out.data_ptr(), params, T, T, stats=True)
         if i > 0:
             e2e_ms.append(ctx.last_timing().total_ms)
+    if e2e:
+        check(pin_out.numpy().view(np.uint32), ticks, info, f"{G}^3 x {T} ticks, host-buffer run")
     barrier(pg, local)
 
     tot_dev = max_over_ranks(pg, local, sum(dev_ms))
     tot_e2e = max_over_ranks(pg, local, sum(e2e_ms)) if e2e_ms else float("nan")
     tot_tick = max_over_ranks(pg, local, sum(tick_ms))
-    value = world * cells_per_step * args.steps / (tot_dev / 1e3)
-    e2e_value = world * cells_per_step * args.steps / (tot_e2e / 1e3)
-    per_launch_s = (tot_tick / 1e3) / (T * args.steps)
+    value = world * cells_per_step * steps / (tot_dev / 1e3)
+    per_launch_s = (tot_tick / 1e3) / (T * steps)
     alg_bytes = G ** 3  # 1 byte per cell update: 0.5 B read + 0.5 B written
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / per_launch_s / 1e9
-    traffic = committed_traffic(f"stream_tick_{G}")
     line = {
         "metric": "cell-updates/s",
         "value": value,
         "unit": "cell-updates/s",
         "n_gpus": world,
-        "steps": args.steps,
-        "warmup": args.warmup,
-        "ms_per_step": tot_dev / args.steps,
+        "steps": steps,
+        "warmup": warmup,
+        "ms_per_step": tot_dev / steps,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
@@ -295,32 +423,120 @@ def large_workload(args, world, rank, local, pg):
                    "l2": "256 MiB buffer written between timed steps (a step is one whole run; within a run each "
                          "tick reads the previous tick's output)",
                    "tick_kernel": ("compiled for the rule at run time (NVRTC, cached; cave_prepare_rule took "
-                                   f"{prep_s:.2f} s before the warm-up)") if specialised else
-                                  "generic (rule read at run time)"},
+                                   f"{prep_s:.2f} s before the warm-up), "
+                                   + ("two ticks per launch" if pairs else "one tick per launch"))
+                                  if specialised else "generic (rule read at run time), one tick per launch"},
         "tick_kernel_us": per_launch_s * 1e6,
+        "ticks_per_launch": 2 if pairs else 1,
         "convert_ms_per_step": sum(conv_ms) / len(conv_ms),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "traffic": traffic,
-                     "note": "algorithmic bytes = 1 B per cell update (packed 4-bit state read once, written once)"},
-        "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": int(words * 4),
-                "d2h_bytes_per_step": int(words * 4 + T * 48)},
+                     "peak_kind": peak_kind, "traffic": committed_traffic(f"stream_tick_{G}"),
+                     "note": "algorithmic bytes = 1 B per cell update (packed 4-bit state read once, written once "
+                             "per tick); achieved = G^3 B x ticks / tick-loop time (CUDA events on the library's "
+                             "stream)" + ("; two ticks per launch: the grid crosses HBM once per two ticks, so the "
+                                          "achieved rate can exceed the copy bandwidth and `traffic` (DRAM bytes "
+                                          "per launch, ncu) is about half the algorithmic bytes of its two ticks"
+                                          if pairs else "")},
+        "parity": ({"ok": True, "checked": f"last timed run{' and last end-to-end run' if e2e else ''}: every cell, "
+                                          f"every tick's statistics and the GridInfo equal "
+                                          f"tests/golden/large_fixtures.json ({G}^3, {T} ticks)"}
+                   if want else {"ok": None, "checked": f"no oracle fixture for {G}^3 x {T} ticks"}),
         "gpu_launches": int(sum_over_ranks(pg, local, launches)),
         "clocks": clocks,
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        params_np = np.array([params.birthAndMaxCellStateRules, params.survivalAndNeighborhoodRules, 0],
-                             dtype=np.uint64)
-        line["cpu_baseline"] = cpu_baseline_large(G, init_host, params_np)
+    if e2e:
+        line["e2e"] = {"value": world * cells_per_step * steps / (tot_e2e / 1e3), "unit": "cell-updates/s",
+                       "h2d_bytes_per_step": int(words * 4), "d2h_bytes_per_step": int(words * 4 + T * 48)}
+    if rank == 0 and world == 1 and cpu and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_grid(G, init_host, LARGE_RULE, T, single=G <= 512,
+                                                 budget_s=10.0 if G <= 512 else 12.0)
     g.close()
     ctx.close()
     return line
 
 
+# ----------------------------------------------------------------------------- config 1
+def plain49_workload(args, world, rank, local, pg, steps, warmup):
+    """The plain single simulation: 49^3, FE, C = 4, survive {5,6,7} birth {6,7}, 30% fill of
+    the centred 16^3 box, seed 0, 20 ticks, statistics every tick -- through the plain path
+    (cave_step: one launch per tick, the reference's per-tick dispatch), the streaming path
+    (cave_run) and the resident kernel (a batch of this one simulation, all ticks on chip)."""
+    import cave_b200 as cb
+
+    G, T = WORKLOADS["plain49"]
+    thr = cb.threshold_from_fill(0.30)
+    params = cb.make_params(*PLAIN_RULE)
+    ctx = cb.Context(local)
+    ctx.set_timing(True)
+    want = fixture("large_fixtures.json").get("49", {}).get("checkpoints", {}).get(str(T))
+    out = {"workload": "49^3 FE, C=4 (maxCellState 3), survive {5,6,7} birth {6,7}, 30% fill of a centred 16^3 box, "
+                       "seed 0, 20 ticks, statistics every tick", "unit": "sims/s"}
+    launches = 0
+    with cb.Grid(ctx, G, G, G) as g, ClockSampler(local) as clk:
+        g.seed_threshold((16, 16, 16), thr, 0, 3)
+        init = g.download()
+        for path in ("plain", "streaming"):
+            ms = []
+            for i in range(warmup + steps):
+                g.upload(init)
+                if path == "plain":
+                    ticks = g.step(params, T)
+                    info = None
+                else:
+                    ticks, info = g.run(params, T, T)
+                t = ctx.last_timing()
+                if i >= warmup:
+                    ms.append(t.tick_ms)
+                    launches += t.launches
+            if want:
+                rec = cb.tick_records(ticks)
+                require(hashlib.sha256(rec.tobytes()).hexdigest() == want["ticks_sha256"],
+                        f"plain 49^3 ({path}): per-tick statistics")
+                require(sha256_u32(g.download()) == want["cells_sha256"], f"plain 49^3 ({path}): cells")
+                if info is not None:
+                    require(list(info.as_tuple()) == want["gridinfo"], f"plain 49^3 ({path}): GridInfo")
+            dev = max_over_ranks(pg, local, statistics.median(ms))
+            out[path] = {"sims_per_s": 1e3 / dev, "cell_updates_per_s": G ** 3 * T / (dev / 1e3),
+                         "us_per_tick": dev * 1e3 / T, "ms_per_sim": dev,
+                         "how": "cave_step: one launch per tick" if path == "plain" else
+                                "cave_run: layout conversion, one tick launch per tick, deferred fold"}
+        # resident: one simulation in one CTA's shared memory for all its ticks
+        ms = []
+        for i in range(warmup + steps):
+            with cb.Batch(ctx) as b:
+                ix = b.add_init(G, G, G, init)
+                b.add_sims([cb.SimDesc(params, ix, T, 0, 0)])
+                b.launch()
+                r = b.results_array()
+                t = ctx.last_timing()
+            if i >= warmup:
+                ms.append(t.tick_ms)
+                launches += t.launches
+        if want:
+            require(list(r[0]["info"]) == want["gridinfo"], "plain 49^3 (resident): GridInfo")
+        dev = max_over_ranks(pg, local, statistics.median(ms))
+        out["resident"] = {"sims_per_s": 1e3 / dev, "cell_updates_per_s": G ** 3 * T / (dev / 1e3),
+                           "us_per_tick": dev * 1e3 / T, "ms_per_sim": dev,
+                           "how": "a batch of this one simulation: one persistent launch, grid in shared memory"}
+    out["clocks"] = clk.summary()
+    out["gpu_launches"] = launches
+    out["parity"] = ({"ok": True, "checked": "plain and streaming: every cell after tick 20, every tick's statistics; "
+                                             "streaming and resident: GridInfo; vs tests/golden/large_fixtures.json"}
+                     if want else {"ok": None, "checked": "no oracle fixture"})
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_grid(G, init, PLAIN_RULE, T, budget_s=3.0)
+        # per simulation of 20 ticks
+        cpu["sims_per_s"] = cpu["value"] / (G ** 3 * T)
+        cpu["single_thread"]["sims_per_s"] = cpu["single_thread"]["value"] / (G ** 3 * T)
+        out["cpu_baseline"] = cpu
+    ctx.close()
+    return out
+
+
+# ----------------------------------------------------------------------------- config 3
 def sweep_descs(G, seeds, cs_values, rank=0, world=1, stride=1):
     """The config-3 sweep: FE neighbourhood, every survive/birth set with <= 2 bits (171 each),
     C in cs_values (maxCellState = C - 1), `seeds` seeds; sims of this rank's shard."""
-    import numpy as np
-
     import cave_b200 as cb
 
     n_masks = 171
@@ -345,9 +561,7 @@ def sweep_descs(G, seeds, cs_values, rank=0, world=1, stride=1):
     return np.ascontiguousarray(mine[::stride])
 
 
-def sweep_workload(args, world, rank, local, pg):
-    import numpy as np
-
+def sweep_workload(args, world, rank, local, pg, steps, warmup):
     import cave_b200 as cb
 
     G, T = WORKLOADS["sweep49"]
@@ -369,21 +583,19 @@ def sweep_workload(args, world, rank, local, pg):
     if args.stride > 1:
         full = np.ascontiguousarray(full[::args.stride])
     warm = np.ascontiguousarray(full[::32])
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         with make_batch() as b:
             b.add_sims_array(warm, max_rule_bits=2)
             b.launch()
             b.results_array()
     barrier(pg, local)
-    kern_ms, tot_ms, wall, cats, ticks, launches = [], [], [], None, 0, 0
+    kern_ms, tot_ms, cats, ticks, launches, res = [], [], None, 0, 0, None
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
+        for _ in range(steps):
             with make_batch() as b:
-                t0 = time.perf_counter()
                 b.add_sims_array(full, max_rule_bits=2)
                 b.launch()
                 res = b.results_array()
-                wall.append(time.perf_counter() - t0)
                 t = ctx.last_timing()
                 kern_ms.append(t.tick_ms)
                 tot_ms.append(t.total_ms)
@@ -392,6 +604,20 @@ def sweep_workload(args, world, rank, local, pg):
             ticks = int(res["info"][:, 2].sum())
         barrier(pg, local)
     clocks = clk.summary()
+    # parity: every 64th simulation of the sweep against the oracle fixture
+    fx = fixture("sweep49_fixture.json")
+    parity = {"ok": None, "checked": "not checked (sharded or strided run, or no fixture)"}
+    if fx and world == 1 and args.stride == 1:
+        sample = res[::fx["stride"]]
+        rec = cb.result_records(sample, np.asarray(full["tag"][::fx["stride"]], dtype=np.uint64))
+        blocks = [hashlib.sha256(rec[i:i + fx["block"]].tobytes()).hexdigest()
+                  for i in range(0, rec.shape[0], fx["block"])]
+        bad = [i for i, (a, b) in enumerate(zip(blocks, fx["block_sha256"])) if a != b]
+        require(len(blocks) == len(fx["block_sha256"]) and not bad,
+                f"sweep49: result blocks {bad[:8]} of every-64th-simulation sample differ from the oracle fixture")
+        parity = {"ok": True, "checked": f"every {fx['stride']}th simulation ({rec.shape[0]}): GridInfo, category, "
+                                         f"population, active ticks, changed cells, bounding box equal "
+                                         f"tests/golden/sweep49_fixture.json"}
     n_all = sum_over_ranks(pg, local, float(full.size))
     kern = max_over_ranks(pg, local, sum(kern_ms) / len(kern_ms))
     tot = max_over_ranks(pg, local, sum(tot_ms) / len(tot_ms))
@@ -405,15 +631,14 @@ def sweep_workload(args, world, rank, local, pg):
             with make_batch() as b:
                 b.add_sims_array(sample, max_rule_bits=2)
                 dev_s = b.run_plain(slots)
-                r = b.results_array()
             v = sample.size / dev_s
             plain[f"slots{slots}_sims_per_s"] = v
             best = v if best is None else max(best, v)
         plain["best_sims_per_s"] = best
         plain["sample"] = f"{sample.size} simulations (every 997th of the sweep)"
     line = {
-        "metric": "search sims/s", "value": sims_s, "unit": "sims/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": kern, "higher_is_better": True, "scaling": "strong",
+        "metric": "search sims/s", "value": sims_s, "unit": "sims/s", "n_gpus": world, "steps": steps,
+        "warmup": warmup, "ms_per_step": kern, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "u4 (packed nibble states, bit-sliced integer logic)",
         "data": "synthetic: reference cell hash, 30% fill of a centred 16^3 box, seeds 0..31",
         "config": {"workload": f"49^3 FE sweep: 171 x 171 rules (<= 2 bits) x C in {{2,3,4,5}} x 32 seeds, "
@@ -426,6 +651,7 @@ def sweep_workload(args, world, rank, local, pg):
         "categories": {"viable": int(cats[0]), "possible": int(cats[1]), "unviable": int(cats[2])},
         "plain_path": plain,
         "batched_over_plain": (sims_s / plain["best_sims_per_s"]) if plain else None,
+        "parity": parity,
         "e2e": {"value": n_all / (tot / 1e3), "unit": "sims/s", "h2d_bytes_per_step": int(full.size * 16),
                 "d2h_bytes_per_step": int(full.size * cb.SIM_RESULT_DTYPE.itemsize)},
         "gpu_launches": int(sum_over_ranks(pg, local, launches)),
@@ -436,9 +662,15 @@ def sweep_workload(args, world, rank, local, pg):
                       "alu_pipe_frac": committed_profile_value("resident_sweep49", "alu_pipe_frac"),
                       "source": "ncu --set full, profiles/resident_sweep49.md"},
     }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        sample = sweep_descs(G, seeds, cs_values, stride=997)[:16 * cores]
+        items = [(int((int(d["birth"]) >> 60) & 0xF) + 1, int(d["init"]) % seeds,
+                  int((int(d["survival"]) & 0xFFFFFFFF) - 1), int((int(d["birth"]) & 0xFFFFFFFF) - 1))
+                 for d in sample]
+        line["cpu_baseline"] = cpu_baseline_sims(_cpu_sweep_sim, items, "every 997th simulation of the sweep")
     ctx.close()
     return line
-
 
 
 # ----------------------------------------------------------------------------- config 4 / 5 inputs
@@ -471,7 +703,12 @@ def uneven_sims(n, seed=20261203):
     return out
 
 
-def uneven_workload(args, world, rank, local, pg):
+def uneven_spec_digest(sims):
+    keys = ("edge", "flags", "maxcs", "birth", "survival", "ticks", "fill", "seed")
+    return hashlib.sha256(json.dumps([[s[k] for k in keys] for s in sims]).encode()).hexdigest()
+
+
+def uneven_workload(args, world, rank, local, pg, steps, warmup):
     import cave_b200 as cb
 
     sims = uneven_sims(args.sims)
@@ -492,9 +729,9 @@ def uneven_workload(args, world, rank, local, pg):
         return b
 
     autotune = not args.no_autotune
-    tune_ms = 0.0
     t0 = time.perf_counter()
-    for _ in range(args.warmup):
+    plan = None
+    for _ in range(warmup):
         with make_batch(mine, autotune) as b:
             b.launch()
             b.results_array()
@@ -502,9 +739,10 @@ def uneven_workload(args, world, rank, local, pg):
     tune_wall = time.perf_counter() - t0
     barrier(pg, local)
     kern_ms, tot_ms, wall = [], [], []
-    updates, launches = 0, 0
+    updates, launches, res = 0, 0, None
+    vol = np.array([s["edge"] ** 3 for s in mine], dtype=np.int64)
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
+        for _ in range(steps):
             with make_batch(mine, autotune) as b:
                 w0 = time.perf_counter()
                 b.launch()
@@ -515,11 +753,20 @@ def uneven_workload(args, world, rank, local, pg):
                 tot_ms.append(t.total_ms)
                 launches += t.launches
                 plan = b.plan()
-            vol = np.array([s["edge"] ** 3 for s in mine], dtype=np.int64)
             updates = int((res["info"][:, 2].astype(np.int64) * vol).sum())
-            assert int(res["error"].max(initial=0)) == 0
+            require(int(res["error"].max(initial=0)) == 0, "uneven: a simulation raised an error flag")
         barrier(pg, local)
     clocks = clk.summary()
+    fx = fixture("engine_fixture.json").get("uneven", {})
+    parity = {"ok": None, "checked": "not checked (sharded run, another batch size, or no fixture)"}
+    if fx and world == 1 and len(sims) == fx["sims"] and uneven_spec_digest(sims) == fx["spec_sha256"]:
+        rec = cb.result_records(res, np.arange(len(sims)))
+        blocks = [hashlib.sha256(rec[i:i + fx["block"]].tobytes()).hexdigest()
+                  for i in range(0, rec.shape[0], fx["block"])]
+        bad = [i for i, (a, b) in enumerate(zip(blocks, fx["block_sha256"])) if a != b]
+        require(not bad, f"uneven2048: result blocks {bad[:8]} differ from the oracle fixture")
+        parity = {"ok": True, "checked": f"all {len(sims)} simulations: GridInfo, category, population, active ticks, "
+                                         f"changed cells, bounding box equal tests/golden/engine_fixture.json"}
     kern = max_over_ranks(pg, local, sum(kern_ms) / len(kern_ms))
     tot = max_over_ranks(pg, local, sum(tot_ms) / len(tot_ms))
     n_all = sum_over_ranks(pg, local, float(len(mine)))
@@ -538,13 +785,13 @@ def uneven_workload(args, world, rank, local, pg):
             b.launch()
             rb = b.results_array()
             tb = ctx.last_timing().tick_ms / 1e3
-        assert np.array_equal(rb["info"], r["info"]), "plain and batched paths disagree"
+        require(np.array_equal(rb["info"], r["info"]), "uneven: plain and batched paths disagree")
         plain = {"sample": f"{len(sample)} simulations (every 64th)", "plain_sims_per_s": len(sample) / dev_s,
                  "plain_cell_updates_per_s": upd_s / dev_s, "batched_sims_per_s_same_sample": len(sample) / tb,
                  "batched_cell_updates_per_s_same_sample": upd_s / tb, "batched_over_plain_same_sample": dev_s / tb}
     line = {
         "metric": "search sims/s", "value": n_all / (kern / 1e3), "unit": "sims/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": kern, "higher_is_better": True,
+        "steps": steps, "warmup": warmup, "ms_per_step": kern, "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "u4 (packed nibble states, bit-sliced integer logic)",
         "data": "synthetic: reference cell hash, 20-50% fill of the whole grid, seeds 0..2047",
         "config": {"workload": f"uneven batch: {len(sims)} simulations, edges {{33,49,65,97,129,193}}, F/FE/Moore, "
@@ -556,12 +803,15 @@ def uneven_workload(args, world, rank, local, pg):
         "plan": plan,
         "autotune_and_warmup_wall_s": tune_wall,
         "plain_path": plain,
+        "parity": parity,
         "e2e": {"value": n_all / (tot / 1e3), "unit": "sims/s", "h2d_bytes_per_step": int(len(mine) * 40),
                 "d2h_bytes_per_step": int(len(mine) * cb.SIM_RESULT_DTYPE.itemsize)},
         "host_wall_s_per_step": sum(wall) / len(wall),
         "gpu_launches": int(sum_over_ranks(pg, local, launches)),
         "clocks": clocks,
     }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sims(_cpu_uneven_sim, sims[::64], "every 64th simulation of the batch")
     ctx.close()
     return line
 
@@ -598,16 +848,18 @@ def serve_requests(n, rate, seed=20261204):
     return out
 
 
-def serve_workload(args, world, rank, local, pg):
+def serve_workload(args, world, rank, local, pg, rate=None, nreq=None):
     import cave_b200 as cb
 
-    reqs = serve_requests(args.requests, args.rate)[rank::world]
+    rate = rate or args.rate
+    nreq = nreq or args.requests
+    reqs = serve_requests(nreq, rate)[rank::world]
     ctx = cb.Context(local)
     budget = 120 * 10 ** 9
     total_sims = sum(r.size for _, r in reqs)
 
     def run(srv, timed_arrivals):
-        ids, lat = {}, []
+        ids, lat, by_id = {}, [], {}
         t0 = time.perf_counter()
         for t_arr, r in reqs:
             if timed_arrivals:
@@ -616,29 +868,32 @@ def serve_workload(args, world, rank, local, pg):
                     time.sleep(d)
             ids[srv.submit(r)] = r.size
         done = 0
-        upd = 0
         while done < len(ids):
             for rid in srv.poll():
-                res, l = srv.fetch(rid)
-                assert int(res["error"].max(initial=0)) == 0
-                lat.append(l)
+                res, lt = srv.fetch(rid)
+                require(int(res["error"].max(initial=0)) == 0, "serve: a simulation raised an error flag")
+                lat.append(lt)
+                by_id[rid] = res
                 done += 1
             time.sleep(0.0005)
         span = time.perf_counter() - t0
-        st = srv.stats()
-        return span, sorted(lat), st
+        return span, sorted(lat), srv.stats(), [by_id[i] for i in sorted(by_id)]
 
     with cb.Server(ctx, hbm_budget=budget, autotune=False) as srv:
-        warm = serve_requests(2, args.rate, seed=7)
+        warm = serve_requests(2, rate, seed=7)
         for _, r in warm:
             srv.wait(srv.submit(r), 600.0)
-        for rid in srv.poll():
+        for _ in srv.poll():
             pass
     with cb.Server(ctx, hbm_budget=budget) as srv, ClockSampler(local) as clk:
-        span_served, lat, st_served = run(srv, True)
+        span_served, lat, st_served, res_served = run(srv, True)
     clocks = clk.summary()
     with cb.Server(ctx, hbm_budget=budget) as srv:
-        span_off, _, st_off = run(srv, False)
+        span_off, _, st_off, res_off = run(srv, False)
+    # every simulation's result is the same in the served mix as in the offline run
+    same = all(np.array_equal(cb.result_records(a, np.zeros(a.size)), cb.result_records(b, np.zeros(b.size)))
+               for a, b in zip(res_served, res_off))
+    require(same, "serve: a result differs between the served stream and the offline run")
 
     def pct(p):
         return lat[min(len(lat) - 1, int(p * (len(lat) - 1) + 0.5))] if lat else None
@@ -651,7 +906,7 @@ def serve_workload(args, world, rank, local, pg):
         "steps": 1, "warmup": 1, "ms_per_step": span_served * 1e3, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "u4 (packed nibble states, bit-sliced integer logic)",
         "data": "synthetic: Poisson request stream, reference cell hash seeding",
-        "config": {"workload": f"served: {len(reqs)} requests, Poisson {args.rate}/s, 1-256 sims each, edge 32..256, "
+        "config": {"workload": f"served: {len(reqs)} requests, Poisson {rate}/s, 1-256 sims each, edge 32..256, "
                                f"ticks 10..500, F/FE/Moore, C 2..16", "requests": len(reqs), "simulations": total_sims,
                    "hbm_budget_bytes": budget, "arrival_window_s": arrival_span},
         "latency_p50_s": pct(0.50), "latency_p99_s": pct(0.99),
@@ -660,6 +915,8 @@ def serve_workload(args, world, rank, local, pg):
         "served_span_s": span_served, "offline_span_s": span_off, "peak_hbm_bytes": st_served.peakBytes,
         "tick_launches": st_served.tickLaunches, "resident_launches": st_served.residentLaunches,
         "rounds": st_served.rounds,
+        "parity": {"ok": True, "checked": "every simulation's result in the served stream equals the offline run's "
+                                          "(all requests submitted at once)"},
         "gpu_launches": int(st_served.tickLaunches + st_served.residentLaunches + st_served.rounds),
         "clocks": clocks,
         "e2e": {"value": served_ups, "unit": "cell-updates/s", "h2d_bytes_per_step": int(total_sims * 72),
@@ -669,36 +926,55 @@ def serve_workload(args, world, rank, local, pg):
     return line
 
 
+# ----------------------------------------------------------------------------- reference arm
 def reference_arm(args, world, rank, local, pg):
-    """The oracle port of the reference's CPU-free arithmetic on the host cores (no CPU stepping
+    """The oracle port of the reference's shader arithmetic on the host cores (no CPU stepping
     exists in the reference; its GPU path needs Vulkan, which this box does not have)."""
     import oracle as O
 
     if rank != 0:
         return None
-    G, T = WORKLOADS[args.workload]
-    params = O.make_params(15, 0x7, 0x10, 0x18)
+    G, T = WORKLOADS["large512"]
+    params = O.make_params(*LARGE_RULE)
     init = O.seed(G, G, G, random=True, threshold=O.threshold_from_float(0.40), run_seed=0, max_cell_state=15)
     cores = os.cpu_count() or 1
-    ticks_per_step = 1
     cells = init
     for _ in range(args.warmup):
         cells, _ = O.step_fast(G, G, G, params, cells, nthreads=cores)
     t0 = time.perf_counter()
-    for _ in range(args.steps * ticks_per_step):
+    for _ in range(args.steps):
         cells, _ = O.step_fast(G, G, G, params, cells, nthreads=cores)
     el = time.perf_counter() - t0
-    v = G ** 3 * args.steps * ticks_per_step / el
+    v = G ** 3 * args.steps / el
     return {
         "impl": "reference", "metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u4", "data": "synthetic (same seed and fill)",
         "config": {"workload": f"{G}^3 Moore-26, C=16, survive {{4,5}} birth {{5}}; one tick per step "
                                f"(bounded sample of the {T}-tick run)", "grid": [G, G, G]},
-        "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": "port",
+        "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": "port", "cpu_model": cpu_model(),
                          "sample": f"{args.steps} ticks of {G}^3 after {args.warmup} warm-up ticks"},
         "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+
+
+def run_extras(args, world, rank, local, pg):
+    """The other workloads, each as a compact object of the default line."""
+    steps, warmup = max(2, min(args.steps, 3)), 3
+    extra = {}
+
+    def keep(line, drop=("n_gpus", "higher_is_better", "vs_baseline", "dtype")):
+        return {k: v for k, v in line.items() if k not in drop}
+
+    extra["plain49"] = plain49_workload(args, world, rank, local, pg, steps, warmup)
+    for G in (256, 1024):
+        extra[f"large{G}"] = keep(large_workload(args, world, rank, local, pg, G, WORKLOADS[f"large{G}"][1],
+                                                 steps, warmup, e2e=False))
+    extra["sweep49"] = keep(sweep_workload(args, world, rank, local, pg, steps, warmup))
+    extra["uneven2048"] = keep(uneven_workload(args, world, rank, local, pg, 2, warmup))
+    extra["serve200"] = keep(serve_workload(args, world, rank, local, pg, rate=200.0, nreq=64))
+    extra["serve16"] = keep(serve_workload(args, world, rank, local, pg, rate=16.0, nreq=48))
+    return extra
 
 
 def main():
@@ -713,13 +989,19 @@ def main():
         return
     world, rank, local, pg = dist_setup(args)
     if args.workload == "sweep49":
-        line = sweep_workload(args, world, rank, local, pg)
+        line = sweep_workload(args, world, rank, local, pg, args.steps, args.warmup)
     elif args.workload == "uneven2048":
-        line = uneven_workload(args, world, rank, local, pg)
+        line = uneven_workload(args, world, rank, local, pg, args.steps, args.warmup)
     elif args.workload == "serve":
         line = serve_workload(args, world, rank, local, pg)
+    elif args.workload == "plain49":
+        line = plain49_workload(args, world, rank, local, pg, args.steps, args.warmup)
     else:
-        line = large_workload(args, world, rank, local, pg)
+        G, T = WORKLOADS[args.workload]
+        line = large_workload(args, world, rank, local, pg, G, args.ticks or T, args.steps, args.warmup,
+                              e2e=not args.no_e2e)
+        if args.workload == "large512" and not args.no_extra and not args.ticks:
+            line["extra"] = run_extras(args, world, rank, local, pg)
     if rank == 0 and line is not None:
         print(json.dumps(line), flush=True)
     if pg:

@@ -419,6 +419,30 @@ class Grid:
 NOALLOC_SCRATCH_BYTES = 32 << 20
 
 
+def result_records(res: np.ndarray, index) -> np.ndarray:
+    """Simulation results (SIM_RESULT_DTYPE) packed as 18 little-endian uint32 each, the form
+    the golden fixtures hash: index, GridInfo (6), category, population, activeTicks,
+    totalChanged (low, high word), bbox_min (3), bbox_max (3)."""
+    n = res.size
+    out = np.zeros((n, 18), dtype="<u4")
+    out[:, 0] = np.asarray(index, dtype=np.uint64) & 0xFFFFFFFF
+    out[:, 1:7] = res["info"]
+    out[:, 7] = res["category"]
+    out[:, 8] = res["population"]
+    out[:, 9] = res["activeTicks"]
+    out[:, 10] = res["totalChanged"] & 0xFFFFFFFF
+    out[:, 11] = res["totalChanged"] >> 32
+    out[:, 12:15] = res["bbox_min"]
+    out[:, 15:18] = res["bbox_max"]
+    return out
+
+
+def tick_records(ticks) -> np.ndarray:
+    """Per-tick statistics (TickStats list) as a (ticks, 12) little-endian uint32 array: the
+    GridSnapshot (dead, dying, born, surviving), population, changed, bbox_min, bbox_max."""
+    return np.frombuffer(b"".join(bytes(t) for t in ticks), dtype="<u4").reshape(-1, 12)
+
+
 def run_noalloc(ctx: Context, in_ptr, out_ptr, X, Y, Z, params: SimParams, nticks, max_ticks=None, valid=None,
                 max_rule_bits=0, per_tick_ptr=None) -> GridInfo:
     """cave_run_noalloc: the streaming run on caller-owned device buffers (device addresses as

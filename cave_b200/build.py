@@ -33,7 +33,7 @@ def _headers():
 # name each is included under.
 JIT_SOURCES = [(n, os.path.join(CSRC, n)) for n in (
     "cave_stdint.h", "ca_types.h", "ca_core.cuh", "cave_internal.h", "ptx.cuh", "ring.cuh",
-    "stream_common.cuh", "stream_tick.cuh")] + [("../../include/cave_ca.h", os.path.join(HERE, "..", "include", "cave_ca.h"))]
+    "stream_common.cuh", "stream_tick.cuh", "stream_tick2.cuh")] + [("../../include/cave_ca.h", os.path.join(HERE, "..", "include", "cave_ca.h"))]
 _DELIM = "cave_jit_src"
 
 

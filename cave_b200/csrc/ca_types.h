@@ -27,6 +27,16 @@ constexpr int kJitRowsPerThread = 3;
 // kJitRowsPerThread rows (three: about 155) and the ring of rows x strips in shared memory must
 // fit one CTA per SM.
 constexpr int kJitMaxThreads = kJitRowsPerThread == 2 ? 512 : 384;
+// The same for the two-tick kernels (stream_tick2.cuh), which hold two ticks' rolling rows per
+// row of the thread.
+#ifndef CAVE_TICK2_ROWS
+#define CAVE_TICK2_ROWS 2
+#endif
+#ifndef CAVE_TICK2_THREADS
+#define CAVE_TICK2_THREADS 384
+#endif
+constexpr int kJit2RowsPerThread = CAVE_TICK2_ROWS;
+constexpr int kJit2MaxThreads = CAVE_TICK2_THREADS;
 
 constexpr int kMaxTerms = 8;        // capacity of DeviceRule::terms
 constexpr int kMaxSparseTerms = 4;  // the kernels' sparse evaluation handles up to this many terms

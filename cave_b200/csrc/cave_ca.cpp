@@ -82,19 +82,22 @@ SeedSpec make_seed_spec(uint32_t X, uint32_t Y, uint32_t Z, uint32_t sx, uint32_
 }
 
 bool plan_stream(uint32_t sim_index, uint32_t X, uint32_t Y, uint32_t Z, uint32_t target_ctas, uint32_t rows_hint,
-                 StreamPlan& plan, uint32_t spt) {
+                 StreamPlan& plan, uint32_t spt, uint32_t halo, uint32_t max_threads) {
     const uint32_t SX = (X + 31u) / 32u;
-    if (SX == 0 || SX > 32 || Y == 0 || Z == 0 || Y > 65535 || Z > 65535 || spt < 1 || spt > 3) return false;
+    if (SX == 0 || SX > 32 || Y == 0 || Z == 0 || Y > 65535 || Z > 65535 || spt < 1 || spt > 3 || halo < 1 ||
+        halo > 2)
+        return false;
     uint32_t SXp = 1;
     while (SXp < SX) SXp <<= 1;
     const uint32_t step = std::max(1u, 32u / SXp) * spt;  // rows must keep threads a multiple of 32
-    const uint32_t most_threads = spt == 1 ? 1024u : (uint32_t)kJitMaxThreads;
-    uint32_t rows = rows_hint ? rows_hint : std::max((spt == 1 ? 512u : most_threads) * spt / SXp, 3u);
+    const uint32_t most_threads =
+        max_threads ? max_threads : (halo == 2 ? (uint32_t)kJit2MaxThreads : spt == 1 ? 1024u : (uint32_t)kJitMaxThreads);
+    uint32_t rows = rows_hint ? rows_hint : std::max((spt == 1 ? 512u : most_threads) * spt / SXp, 2 * halo + 1);
     rows = std::min(rows, most_threads * spt / SXp);
-    rows = std::min(rows, Y + 2u);
+    rows = std::min(rows, Y + 2u * halo);
     rows = (rows + step - 1) / step * step;
-    if (rows < 3) rows = 3 * step;
-    const uint32_t TY = rows - 2;
+    while (rows < 2 * halo + 1) rows += step;
+    const uint32_t TY = rows - 2 * halo;
     const uint32_t ny = (Y + TY - 1) / TY;
     const uint32_t ty = (Y + ny - 1) / ny;
     uint32_t nz = std::max(1u, target_ctas / ny);
@@ -159,6 +162,7 @@ cave_status cave_ctx_create(int device, cave_ctx** out) {
     if (!c) return CAVE_ERR_OUT_OF_MEMORY;
     c->device = device;
     c->sm_count = prop.multiProcessorCount;
+    c->smem_optin = (int)prop.sharedMemPerBlockOptin;
     if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete c;
         return CAVE_ERR_CUDA;
@@ -424,37 +428,72 @@ cave_status cave_ctx_last_timing(const cave_ctx* ctx, cave_timing* out) {
 // 256), and no closed rule picked the fastest shape for every size measured. So the first long
 // run of a grid shape times a few candidates -- the default and the seven with the least total
 // row work (tiles x rows per tile) at up to 576 threads, the most that keeps two CTAs per SM --
-// for five ticks each and keeps the fastest per context (the default unless another is more than
-// 2% faster: short trials are noisy). With the rule-specialised kernels (kJitRowsPerThread rows
-// per thread) the candidates stay at or below kJitMaxThreads threads. The trial ticks read the run's input
-// copy and write the other one, which tick 0 overwrites, and add to the first tick's statistics
-// slot, which is cleared afterwards; results do not depend on the tile shape.
+// for five launches each and keeps the fastest per context (the default unless another is more
+// than 2% faster: short trials are noisy). With the rule-specialised kernels the candidates stay
+// within those kernels' thread limit (kJitMaxThreads, kJit2MaxThreads) and, for the two-tick
+// kernels, within the shared memory of one CTA. The trial launches read the run's input copy and
+// write the other one, which the first real launch overwrites, and add to the first statistics
+// slots, which are cleared afterwards; results do not depend on the tile shape.
 constexpr uint32_t kTuneMinTicks = 100;
 
-// The plan of one cave_run tile shape: `rows` per CTA (0 = default) at `spt` rows per thread.
-// Generic kernels: `cps` CTAs per SM (default 2). Rule-specialised kernels (kJitRowsPerThread
-// rows per thread, one CTA of up to kJitMaxThreads per SM by registers): as many CTAs per SM as
-// kJitMaxThreads-thread equivalents, unless `cps` was given.
-static bool run_plan(const cave_ctx* ctx, const cave_grid* g, uint32_t rows, uint32_t spt, uint32_t cps,
+// The tick kernels cave_run can use: the library's own (rule read at run time), the
+// rule-specialised single-tick kernels, and the rule-specialised two-tick kernels.
+enum RunKind : uint32_t { kRunGeneric = 0, kRunJit = 1, kRunJitPair = 2 };
+
+static uint32_t kind_spt(uint32_t kind) {
+    return kind == kRunGeneric ? 1u : kind == kRunJit ? (uint32_t)kJitRowsPerThread : (uint32_t)kJit2RowsPerThread;
+}
+static uint32_t kind_halo(uint32_t kind) { return kind == kRunJitPair ? 2u : 1u; }
+static uint32_t kind_max_threads(uint32_t kind) {
+    return kind == kRunGeneric ? 1024u : kind == kRunJit ? (uint32_t)kJitMaxThreads : (uint32_t)kJit2MaxThreads;
+}
+// Dynamic shared memory the two-tick kernels may take (their static share is a few KB).
+static bool pair_smem_fits(const cave_ctx* ctx, const StreamPlan& p) {
+    return tick2_smem_bytes(p.rows, p.SX, p.SXp) + 4096 <= (size_t)ctx->smem_optin;
+}
+
+// The plan of one cave_run tile shape: `rows` per CTA (0 = default) for tick kernels of `kind`.
+// Generic kernels: `cps` CTAs per SM (default 2). Rule-specialised kernels (one CTA of up to
+// their thread limit per SM, by registers): as many CTAs per SM as limit-sized equivalents,
+// unless `cps` was given. Two-tick kernels: rows shrink until the CTA's shared memory fits.
+static bool run_plan(const cave_ctx* ctx, const cave_grid* g, uint32_t rows, uint32_t kind, uint32_t cps,
                      bool cps_given, StreamPlan& plan) {
     const uint32_t sms = (uint32_t)ctx->sm_count;
-    if (spt == 1) return plan_stream(0, g->X, g->Y, g->Z, sms * cps, rows, plan, 1);
-    if (!plan_stream(0, g->X, g->Y, g->Z, sms * (cps_given ? cps : 1u), rows, plan, spt)) return false;
-    if (!cps_given && plan.threads < (uint32_t)kJitMaxThreads)
-        return plan_stream(0, g->X, g->Y, g->Z, sms * ((uint32_t)kJitMaxThreads / plan.threads), plan.rows, plan, spt);
+    const uint32_t spt = kind_spt(kind), halo = kind_halo(kind), most = kind_max_threads(kind);
+    if (kind == kRunGeneric) return plan_stream(0, g->X, g->Y, g->Z, sms * cps, rows, plan, 1);
+    if (!plan_stream(0, g->X, g->Y, g->Z, sms * (cps_given ? cps : 1u), rows, plan, spt, halo)) return false;
+    if (kind == kRunJitPair) {
+        const uint32_t step = std::max(1u, 32u / plan.SXp) * spt;
+        while (!pair_smem_fits(ctx, plan)) {
+            if (plan.rows < 2 * halo + 1 + step) return false;
+            if (!plan_stream(0, g->X, g->Y, g->Z, sms * (cps_given ? cps : 1u), plan.rows - step, plan, spt, halo))
+                return false;
+        }
+    }
+    if (!cps_given && plan.threads < most)
+        return plan_stream(0, g->X, g->Y, g->Z, sms * (most / plan.threads), plan.rows, plan, spt, halo);
     return true;
 }
 
-static std::vector<uint32_t> row_candidates(uint32_t X, uint32_t Y, uint32_t rows0, uint32_t spt) {
+static std::vector<uint32_t> row_candidates(const cave_ctx* ctx, uint32_t X, uint32_t Y, uint32_t rows0,
+                                            uint32_t kind) {
     const uint32_t SX = (X + 31u) / 32u;
     uint32_t SXp = 1;
     while (SXp < SX) SXp <<= 1;
+    const uint32_t spt = kind_spt(kind), halo = kind_halo(kind);
     const uint32_t step = std::max(1u, 32u / SXp) * spt;
-    const uint32_t hi = std::min((spt == 1 ? 576u : (uint32_t)kJitMaxThreads) * spt / SXp, Y + 2u);
+    const uint32_t hi = std::min((kind == kRunGeneric ? 576u : kind_max_threads(kind)) * spt / SXp, Y + 2u * halo);
     std::vector<std::pair<uint64_t, uint32_t>> scored;
-    for (uint32_t r = std::max(3u * step, (rows0 / 2 + step - 1) / step * step); r <= hi; r += step) {
-        if (r == rows0 || r < 3) continue;
-        const uint64_t tiles = (Y + (r - 2) - 1) / (r - 2);
+    for (uint32_t r = std::max((2 * halo + 1) * step, (rows0 / 2 + step - 1) / step * step); r <= hi; r += step) {
+        if (r == rows0 || r < 2 * halo + 1) continue;
+        if (kind == kRunJitPair) {
+            StreamPlan p;
+            p.rows = r;
+            p.SX = SX;
+            p.SXp = SXp;
+            if (!pair_smem_fits(ctx, p)) continue;
+        }
+        const uint64_t tiles = (Y + (r - 2 * halo) - 1) / (r - 2 * halo);
         scored.push_back({tiles * r, r});
     }
     std::sort(scored.begin(), scored.end());
@@ -463,24 +502,46 @@ static std::vector<uint32_t> row_candidates(uint32_t X, uint32_t Y, uint32_t row
     return out;
 }
 
-// Times one candidate plan: one untimed tick then five timed ones (tick index 0 each time).
-static cudaError_t time_plan(cave_ctx* ctx, cave_grid* g, const DeviceRule& rule, const JitKernels& jk,
+// One launch of cave_run's tick loop: ticks `tick` (and tick + 1 for the two-tick kernels),
+// reading cell copy `sel` (the single-tick kernels take it from the tick's parity).
+static cudaError_t launch_run_tick(cave_ctx* ctx, cave_grid* g, uint32_t kind, const DeviceRule& rule,
+                                   const JitKernels& jk, const StreamPlan& plan, const StreamItem* ditems, bool first,
+                                   bool pdl, uint32_t tick, uint32_t sel) {
+    const uint32_t n = (uint32_t)plan.items.size();
+    const bool dense = plan.SX == plan.SXp;
+    switch (kind) {
+        case kRunJitPair:
+            return launch_stream_tick2_jit(jk.pick2(first, dense), ditems, n, g->sim, g->strips, plan.SX, plan.SXp,
+                                           plan.threads, ctx->stream, pdl, (int)tick, (int)sel);
+        case kRunJit:
+            return launch_stream_tick_jit(jk.pick(first, dense), ditems, n, g->sim, g->strips, plan.SX, plan.SXp,
+                                          plan.threads, ctx->stream, pdl, (int)tick);
+        default:
+            return launch_stream_tick((int)(rule.flags & 7u), (int)rule.nterms, &rule, ditems, n, g->sim, g->strips,
+                                      plan.SX, plan.SXp, plan.threads, ctx->stream, pdl, (int)tick);
+    }
+}
+
+// Times one candidate plan: one untimed launch then five timed ones (tick index 0 each time).
+static cudaError_t time_plan(cave_ctx* ctx, cave_grid* g, uint32_t kind, const DeviceRule& rule, const JitKernels& jk,
                              const StreamPlan& plan, StreamItem* ditems, cudaEvent_t e0, cudaEvent_t e1, float* ms) {
     cudaError_t e = cudaMemcpyAsync(ditems, plan.items.data(), sizeof(StreamItem) * plan.items.size(),
                                     cudaMemcpyHostToDevice, ctx->stream);
     for (int i = 0; i < 6 && e == cudaSuccess; i++) {
         if (i == 1) e = cudaEventRecord(e0, ctx->stream);
-        if (e != cudaSuccess) break;
-        e = jk ? launch_stream_tick_jit(jk.pick(true, plan.SX == plan.SXp), ditems, (uint32_t)plan.items.size(),
-                                        g->sim, g->strips, plan.SX, plan.SXp, plan.threads, ctx->stream, i > 0, 0)
-               : launch_stream_tick((int)(rule.flags & 7u), (int)rule.nterms, &rule, ditems,
-                                    (uint32_t)plan.items.size(), g->sim, g->strips, plan.SX, plan.SXp, plan.threads,
-                                    ctx->stream, i > 0, 0);
+        if (e == cudaSuccess) e = launch_run_tick(ctx, g, kind, rule, jk, plan, ditems, true, i > 0, 0, 0);
     }
     if (e == cudaSuccess) e = cudaEventRecord(e1, ctx->stream);
     if (e == cudaSuccess) e = cudaEventSynchronize(e1);
     if (e == cudaSuccess) e = cudaEventElapsedTime(ms, e0, e1);
     return e;
+}
+
+// cave_run's tick kernels by default use two ticks per launch when the rule-specialised kernels
+// are ready and the run has two ticks or more; CAVE_TICK2=0 keeps one tick per launch.
+static bool pair_ticks_enabled() {
+    const char* v = std::getenv("CAVE_TICK2");
+    return !(v && (!std::strcmp(v, "0") || !std::strcmp(v, "off")));
 }
 
 static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* host_out, const cave_sim_params* params,
@@ -537,18 +598,22 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
     record(ctx, 1);
     if (e == cudaSuccess) e = launch_nib_to_strips(g->nib[g->cur], g->strips, g->X, g->Y, g->Z, ctx->stream);
     record(ctx, 2);
-    // the rule-specialised kernel when one is ready (jit.h), else the generic one
+    // the rule-specialised kernels when they are ready (jit.h), else the generic one; with them
+    // two ticks per launch unless disabled (the run's first launch counts every statistic; later
+    // ones leave the zero cells to the fold)
     const JitMode jm = jit_mode();
-    // (its first tick counts every statistic; later ticks leave the zero cells to the fold)
     const JitKernels jk = nticks ? jit_stream_kernel(jit_key(s.rule), jm, (uint64_t)g->X * g->Y * g->Z >= kJitMinCells)
                                  : JitKernels{};
-    // tile shape: an override, the context's earlier choice for this shape, or a timing pass;
-    // the rule-specialised kernels take kJitRowsPerThread rows per thread
-    const uint32_t spt = jk ? (uint32_t)kJitRowsPerThread : 1u;
-    if (e == cudaSuccess && !run_plan(ctx, g, rows_hint, spt, cps, env_cps != nullptr, plan))
-        return set_error(ctx, CAVE_ERR_INTERNAL, "streaming plan failed");
+    uint32_t kind = !jk ? kRunGeneric : (nticks >= 2 && jk.pair[0] && pair_ticks_enabled()) ? kRunJitPair : kRunJit;
+    if (e == cudaSuccess && !run_plan(ctx, g, rows_hint, kind, cps, env_cps != nullptr, plan)) {
+        if (kind != kRunJitPair) return set_error(ctx, CAVE_ERR_INTERNAL, "streaming plan failed");
+        kind = kRunJit;  // the grid's rows do not fit the two-tick kernel's shared memory
+        if (!run_plan(ctx, g, rows_hint, kind, cps, env_cps != nullptr, plan))
+            return set_error(ctx, CAVE_ERR_INTERNAL, "streaming plan failed");
+    }
+    // tile shape: an override, the context's earlier choice for this shape, or a timing pass
     if (e == cudaSuccess && !rows_hint && nticks >= kTuneMinTicks && (uint64_t)g->X * g->Y * g->Z >= kJitMinCells) {
-        const TuneKey key{g->X, g->Y, g->Z, (d.flags & 7u) + (jk ? 8u : 0u)};
+        const TuneKey key{g->X, g->Y, g->Z, (d.flags & 7u) + 8u * kind};
         uint32_t rows = 0;
         {
             std::lock_guard<std::mutex> lk(ctx->tune_mu);
@@ -558,9 +623,9 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
         if (!rows) {
             std::vector<StreamPlan> cands;
             size_t most = 0;
-            for (uint32_t r : row_candidates(g->X, g->Y, plan.rows, spt)) {
+            for (uint32_t r : row_candidates(ctx, g->X, g->Y, plan.rows, kind)) {
                 StreamPlan c;
-                if (!run_plan(ctx, g, r, spt, cps, env_cps != nullptr, c)) continue;
+                if (!run_plan(ctx, g, r, kind, cps, env_cps != nullptr, c)) continue;
                 most = std::max(most, c.items.size());
                 cands.push_back(std::move(c));
             }
@@ -572,7 +637,7 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
             float best = 1e30f;
             for (const StreamPlan& c : cands) {
                 float ms = 0;
-                if (e == cudaSuccess) e = time_plan(ctx, g, s.rule, jk, c, titems, e0, e1, &ms);
+                if (e == cudaSuccess) e = time_plan(ctx, g, kind, s.rule, jk, c, titems, e0, e1, &ms);
                 if (e == cudaSuccess && c.rows == plan.rows) ms *= 0.98f;  // a challenger must beat the default by 2%
                 if (e == cudaSuccess && ms < best) {
                     best = ms;
@@ -582,34 +647,58 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
             if (e0) cudaEventDestroy(e0);
             if (e1) cudaEventDestroy(e1);
             cudaFree(titems);
-            if (e == cudaSuccess) e = cudaMemsetAsync(dtt, 0, sizeof(TickTotals), ctx->stream);
+            if (e == cudaSuccess)
+                e = cudaMemsetAsync(dtt, 0, sizeof(TickTotals) * (kind == kRunJitPair ? 2 : 1), ctx->stream);
             if (e == cudaSuccess) {
                 std::lock_guard<std::mutex> lk(ctx->tune_mu);
                 ctx->run_rows[key] = rows;
             }
         }
-        if (e == cudaSuccess && rows != plan.rows && !run_plan(ctx, g, rows, spt, cps, env_cps != nullptr, plan))
+        if (e == cudaSuccess && rows != plan.rows && !run_plan(ctx, g, rows, kind, cps, env_cps != nullptr, plan))
             return set_error(ctx, CAVE_ERR_INTERNAL, "tile shape chosen by the timing pass could not be planned");
     }
-    if (e == cudaSuccess) e = cudaMalloc(&ditems, sizeof(StreamItem) * plan.items.size());
+    // an odd tick count with the two-tick kernels: tick 0 alone first, with the single-tick plan
+    StreamPlan plan1;
+    const bool lead = kind == kRunJitPair && (nticks & 1u);
+    if (e == cudaSuccess && lead && !run_plan(ctx, g, 0, kRunJit, cps, env_cps != nullptr, plan1))
+        return set_error(ctx, CAVE_ERR_INTERNAL, "streaming plan failed");
+    const size_t n_main = plan.items.size(), n_lead = lead ? plan1.items.size() : 0;
+    if (e == cudaSuccess) e = cudaMalloc(&ditems, sizeof(StreamItem) * (n_main + n_lead));
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(ditems, plan.items.data(), sizeof(StreamItem) * plan.items.size(), cudaMemcpyHostToDevice,
+        e = cudaMemcpyAsync(ditems, plan.items.data(), sizeof(StreamItem) * n_main, cudaMemcpyHostToDevice,
                             ctx->stream);
-    for (uint32_t t = 0; t < nticks && e == cudaSuccess; t++)
-        e = jk ? launch_stream_tick_jit(jk.pick(t == 0, plan.SX == plan.SXp), ditems, (uint32_t)plan.items.size(), g->sim,
-                                        g->strips, plan.SX, plan.SXp, plan.threads, ctx->stream, true, (int)t)
-               : launch_stream_tick((int)(d.flags & 7u), (int)s.rule.nterms, &s.rule, ditems,
-                                    (uint32_t)plan.items.size(), g->sim, g->strips, plan.SX, plan.SXp, plan.threads,
-                                    ctx->stream, true, (int)t);
+    if (e == cudaSuccess && lead)
+        e = cudaMemcpyAsync(ditems + n_main, plan1.items.data(), sizeof(StreamItem) * n_lead, cudaMemcpyHostToDevice,
+                            ctx->stream);
+    // The tick launches. A launch reads cell copy `sel` and writes the other one.
+    uint32_t sel = 0, launches = 0;
+    if (kind == kRunJitPair) {
+        uint32_t t = 0;
+        if (lead && e == cudaSuccess) {
+            e = launch_run_tick(ctx, g, kRunJit, s.rule, jk, plan1, ditems + n_main, true, true, 0, 0);
+            t = 1;
+            sel = 1;
+            launches++;
+        }
+        for (; t + 1 < nticks && e == cudaSuccess; t += 2) {
+            e = launch_run_tick(ctx, g, kind, s.rule, jk, plan, ditems, t == 0, true, t, sel);
+            sel ^= 1u;
+            launches++;
+        }
+    } else {
+        for (uint32_t t = 0; t < nticks && e == cudaSuccess; t++)
+            e = launch_run_tick(ctx, g, kind, s.rule, jk, plan, ditems, t == 0, true, t, t & 1u);
+        sel = nticks & 1u;
+        launches = nticks;
+    }
     if (e == cudaSuccess && nticks && jk)  // the last tick's population comes from the final grid
-        e = launch_strip_stats(g->strips + (uint64_t)(nticks & 1u) * nstrips, g->Y, g->Z, plan.SX, dtt + (nticks - 1),
+        e = launch_strip_stats(g->strips + (uint64_t)sel * nstrips, g->Y, g->Z, plan.SX, dtt + (nticks - 1),
                                (uint32_t)ctx->sm_count, ctx->stream);
     if (e == cudaSuccess && nticks) e = launch_fold_deferred(g->sim, dtt, nticks, (bool)jk, ctx->stream);
     record(ctx, 3);
-    // Raw stepping never stops early, so the result is in copy (nticks & 1).
+    // Raw stepping never stops early, so the result is in copy `sel`.
     if (e == cudaSuccess)
-        e = launch_strips_to_nib(g->strips + (uint64_t)(nticks & 1u) * nstrips, g->nib[g->cur], g->X, g->Y, g->Z,
-                                 ctx->stream);
+        e = launch_strips_to_nib(g->strips + (uint64_t)sel * nstrips, g->nib[g->cur], g->X, g->Y, g->Z, ctx->stream);
     record(ctx, 4);
     if (e == cudaSuccess && host_out)
         e = cudaMemcpyAsync(host_out, g->nib[g->cur], g->words * 4, cudaMemcpyDeviceToHost, ctx->stream);
@@ -623,7 +712,8 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
     cudaFree(ditems);
     cudaFree(dtt);
     if (e != cudaSuccess) return check_cuda(ctx, e, "cave_run");
-    finish_timing(ctx, nticks, nticks + (jk ? 4 : 3), true);
+    finish_timing(ctx, nticks, launches + (jk ? 4 : 3), true);
+    ctx->last_run_kind = kind;
     if (back.error & kErrWaitTimeout) return set_error(ctx, CAVE_ERR_TIMEOUT, "streaming kernel: bulk-copy wait timed out");
     if (back.error) return set_error(ctx, CAVE_ERR_INTERNAL, "streaming kernel raised an error flag");
     if (back.tick != nticks) return set_error(ctx, CAVE_ERR_INTERNAL, "streaming run stopped early");

@@ -44,6 +44,8 @@ struct cave_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     int sm_count = 148;
+    int smem_optin = 227 * 1024;  // largest shared memory one CTA may opt in to
+    uint32_t last_run_kind = 0;   // tick kernels of the last cave_run (0 generic, 1 specialised, 2 two-tick)
     std::string last_error;
     std::mutex mu;  // guards last_error
     bool timing = false;
@@ -95,9 +97,12 @@ struct StreamPlan {
 // Builds the work items of simulation `sim_index` with grid X*Y*Z; `target_ctas` is the
 // number of CTAs one tick should spread over (a multiple of the SM count); rows_hint = rows
 // per CTA including the two halo rows (0 = default); spt = rows per thread (1, or 2 for the
-// rule-specialised kernels): threads = rows * SXp / spt, a whole number of warps.
+// rule-specialised kernels): threads = rows * SXp / spt, a whole number of warps. halo: halo rows
+// on each side of a tile (1, or 2 for the two-tick kernels; rows_hint includes them), at most
+// max_threads threads (0 = the kernel's own limit).
 bool plan_stream(uint32_t sim_index, uint32_t X, uint32_t Y, uint32_t Z, uint32_t target_ctas,
-                 uint32_t rows_hint, StreamPlan& plan, uint32_t spt = 1);
+                 uint32_t rows_hint, StreamPlan& plan, uint32_t spt = 1, uint32_t halo = 1,
+                 uint32_t max_threads = 0);
 
 SeedSpec make_seed_spec(uint32_t X, uint32_t Y, uint32_t Z, uint32_t sx, uint32_t sy, uint32_t sz,
                         uint32_t spawnSizeIndex, uint64_t threshold, bool fill_all, uint32_t seed,

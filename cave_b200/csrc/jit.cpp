@@ -39,6 +39,7 @@ namespace {
 // The translation unit NVRTC compiles: the tick kernel body with the rule as constants.
 const char* const kJitUnit = R"cave_unit(
 #include "stream_tick.cuh"
+#include "stream_tick2.cuh"
 namespace cave {
 struct JitRule {
     static constexpr bool kFixed = true;
@@ -68,9 +69,22 @@ CAVE_JIT_KERNEL(cave_stream_tick_jit, true, false)
 CAVE_JIT_KERNEL(cave_stream_tick_jit_derived, false, false)
 CAVE_JIT_KERNEL(cave_stream_tick_jit_dense, true, true)
 CAVE_JIT_KERNEL(cave_stream_tick_jit_dense_derived, false, true)
+#define CAVE_JIT_KERNEL2(NAME, FIRST, DENSE)                                                              \
+    extern "C" __global__ void __launch_bounds__(cave::kJit2MaxThreads, 1)                                 \
+        NAME(const cave::StreamItem* __restrict__ items, cave::StripSim* sims, uint4* pool, uint32_t sxp_log2, \
+             int tick_arg, int src_sel) {                                                                  \
+        cave::stream_tick2_body<CAVE_JIT_NB, cave::JitRule, FIRST, DENSE, cave::kJit2RowsPerThread>(       \
+            items, sims, pool, sxp_log2, tick_arg, src_sel);                                               \
+    }
+CAVE_JIT_KERNEL2(cave_stream_tick2_jit_first, true, false)
+CAVE_JIT_KERNEL2(cave_stream_tick2_jit, false, false)
+CAVE_JIT_KERNEL2(cave_stream_tick2_jit_dense_first, true, true)
+CAVE_JIT_KERNEL2(cave_stream_tick2_jit_dense, false, true)
 )cave_unit";
 const char* const kJitCounting[2] = {"cave_stream_tick_jit", "cave_stream_tick_jit_dense"};
 const char* const kJitDerived[2] = {"cave_stream_tick_jit_derived", "cave_stream_tick_jit_dense_derived"};
+const char* const kJitPairFirst[2] = {"cave_stream_tick2_jit_first", "cave_stream_tick2_jit_dense_first"};
+const char* const kJitPair[2] = {"cave_stream_tick2_jit", "cave_stream_tick2_jit_dense"};
 
 struct Nvrtc {
     bool ok = false;
@@ -164,7 +178,9 @@ std::vector<std::string> options_for(const JitKey& k) {
     std::snprintf(b[2], sizeof b[2], "-DCAVE_JIT_LUT_S=0x%xu", k.lut_s);
     std::snprintf(b[3], sizeof b[3], "-DCAVE_JIT_LUT_B=0x%xu", k.lut_b);
     // -default-device: the C header's declarations (host functions) are parsed as device ones
-    return {"--gpu-architecture=sm_100a", "-std=c++20", "-default-device", "-lineinfo", b[0], b[1], b[2], b[3]};
+    return {"--gpu-architecture=sm_100a", "-std=c++20", "-default-device", "-lineinfo", b[0], b[1], b[2], b[3],
+            "-DCAVE_TICK2_ROWS=" + std::to_string(kJit2RowsPerThread),
+            "-DCAVE_TICK2_THREADS=" + std::to_string(kJit2MaxThreads)};
 }
 
 // Compiles the kernel for k (or reads it from the disk cache). No device is touched.
@@ -387,6 +403,8 @@ JitKernels jit_stream_kernel(const JitKey& k, JitMode mode, bool start) {
     for (int d = 0; d < 2 && err == cudaSuccess; d++) {
         err = cudaLibraryGetKernel(&e->kern.counting[d], e->lib, kJitCounting[d]);
         if (err == cudaSuccess) err = cudaLibraryGetKernel(&e->kern.derived[d], e->lib, kJitDerived[d]);
+        if (err == cudaSuccess) err = cudaLibraryGetKernel(&e->kern.pair_first[d], e->lib, kJitPairFirst[d]);
+        if (err == cudaSuccess) err = cudaLibraryGetKernel(&e->kern.pair[d], e->lib, kJitPair[d]);
     }
     if (err != cudaSuccess) {
         (void)cudaGetLastError();

@@ -42,11 +42,16 @@ constexpr uint64_t kJitMinCells = 1ull << 21;
 // last tick's population and bounding box.
 // Each comes in two forms, indexed by `dense`: [1] for launches whose rows fill the lanes
 // (strips per row a power of two), [0] for any launch.
+// The two-tick kernels (stream_tick2.cuh) come in the same forms: pair_first for a run's first
+// two ticks, pair for later ones.
 struct JitKernels {
     cudaKernel_t counting[2] = {nullptr, nullptr};
     cudaKernel_t derived[2] = {nullptr, nullptr};
+    cudaKernel_t pair_first[2] = {nullptr, nullptr};
+    cudaKernel_t pair[2] = {nullptr, nullptr};
     explicit operator bool() const { return counting[0] != nullptr; }
     cudaKernel_t pick(bool first_tick, bool dense) const { return first_tick ? counting[dense] : derived[dense]; }
+    cudaKernel_t pick2(bool first_pair, bool dense) const { return first_pair ? pair_first[dense] : pair[dense]; }
 };
 
 // The specialised kernels for `k` if they are ready (loaded into the runtime), else empty. In
@@ -67,6 +72,16 @@ bool jit_compile(const JitKey& k, std::string* log);
 cudaError_t launch_stream_tick_jit(cudaKernel_t k, const StreamItem* items, uint32_t n_items, StripSim* sims,
                                    uint4* pool, uint32_t SX, uint32_t SXp, uint32_t threads, cudaStream_t st,
                                    bool pdl, int tick_arg);
+
+// Launches two ticks (tick_arg, tick_arg + 1) with a specialised two-tick kernel, reading cell
+// copy src_sel and writing the other; `threads` from a plan made with kJit2RowsPerThread rows
+// per thread and two halo rows on each side.
+cudaError_t launch_stream_tick2_jit(cudaKernel_t k, const StreamItem* items, uint32_t n_items, StripSim* sims,
+                                    uint4* pool, uint32_t SX, uint32_t SXp, uint32_t threads, cudaStream_t st,
+                                    bool pdl, int tick_arg, int src_sel);
+
+// Dynamic shared memory of a two-tick launch with `rows` rows per CTA (incl. halo rows).
+size_t tick2_smem_bytes(uint32_t rows, uint32_t SX, uint32_t SXp);
 
 // Process-wide counters behind cave_jit_stats.
 void jit_count_launch();

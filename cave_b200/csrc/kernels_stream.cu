@@ -12,6 +12,7 @@
 #include "jit.h"
 #include "kernels.h"
 #include "stream_tick.cuh"
+#include "stream_tick2.cuh"
 
 namespace cave {
 
@@ -244,6 +245,44 @@ cudaError_t launch_stream_tick_jit(cudaKernel_t k, const StreamItem* items, uint
     cfg.attrs = attr;
     cfg.numAttrs = (pdl && stream_pdl()) ? 1 : 0;
     void* args[] = {(void*)&items, (void*)&sims, (void*)&pool, (void*)&lg, (void*)&tick_arg};
+    const cudaError_t e = cudaLaunchKernelExC(&cfg, (const void*)k, args);
+    if (e == cudaSuccess) jit_count_launch();
+    return e;
+}
+
+size_t tick2_smem_bytes(uint32_t rows, uint32_t SX, uint32_t SXp) { return stream2_smem_bytes(rows, SX, SXp); }
+
+cudaError_t launch_stream_tick2_jit(cudaKernel_t k, const StreamItem* items, uint32_t n_items, StripSim* sims,
+                                    uint4* pool, uint32_t SX, uint32_t SXp, uint32_t threads, cudaStream_t st,
+                                    bool pdl, int tick_arg, int src_sel) {
+    uint32_t lg = 0;
+    while ((1u << lg) < SXp) lg++;
+    const size_t smem = stream2_smem_bytes(kJit2RowsPerThread * threads / SXp, SX, SXp);
+    {
+        static std::mutex mu;
+        static std::map<std::pair<const void*, int>, size_t> configured;
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        std::lock_guard<std::mutex> lock(mu);
+        size_t& c = configured[{(const void*)k, dev}];
+        if (smem > c) {
+            e = cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            c = smem;
+        }
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(n_items);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = (pdl && stream_pdl()) ? 1 : 0;
+    void* args[] = {(void*)&items, (void*)&sims, (void*)&pool, (void*)&lg, (void*)&tick_arg, (void*)&src_sel};
     const cudaError_t e = cudaLaunchKernelExC(&cfg, (const void*)k, args);
     if (e == cudaSuccess) jit_count_launch();
     return e;

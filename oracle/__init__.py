@@ -104,6 +104,8 @@ def lib():
         L.oracle_step.restype = i32
         L.oracle_step_fast.argtypes = [u32, u32, u32, P(u64), P(u64), u32, u32, P(u32), P(u32), P(u32), i32]
         L.oracle_step_fast.restype = i32
+        L.oracle_derived_stats_fast.argtypes = [u32, u32, u32, P(u32), P(u32), P(TickStats), i32]
+        L.oracle_derived_stats_fast.restype = None
         L.oracle_manager.argtypes = [P(u32), P(GridInfo), P(Perms), u64, u64, u32, P(GridInfo), P(Perms)]
         L.oracle_manager.restype = None
         L.oracle_run_sim.argtypes = [u32, u32, u32, P(u64), P(u64), u32, u32, P(u32), u32, i32,
@@ -213,6 +215,17 @@ def step_fast(X, Y, Z, params, cells, valid=None, max_rule_bits=0, nthreads=0):
     if rc != 0:
         raise ValueError(f"oracle_step_fast failed ({rc})")
     return out, snap
+
+
+def step_stats_fast(X, Y, Z, params, cells, valid=None, max_rule_bits=0, nthreads=0):
+    """One tick by the OpenMP step with every per-tick statistic (snapshot and derived), both
+    computed in parallel. Returns (new_cells, TickStats); bit-identical to step()."""
+    out, snap = step_fast(X, Y, Z, params, cells, valid, max_rule_bits, nthreads)
+    st = TickStats()
+    st.dead, st.dying, st.born, st.surviving = (int(v) for v in snap)
+    lib().oracle_derived_stats_fast(X, Y, Z, _u32p(np.ascontiguousarray(cells, dtype=np.uint32)), _u32p(out),
+                                    ctypes.byref(st), nthreads)
+    return out, st
 
 
 def manager(snapshot, info: GridInfo, perms: Perms, max_permutation, survival_end, max_ticks):

@@ -1,7 +1,9 @@
-"""GPU parity of the rule-specialised tick kernel (NVRTC): with CAVE_JIT=sync every cave_run and
-cave_render_step below runs the kernel compiled for its rule, checked bit-exact against the
+"""GPU parity of the rule-specialised tick kernels (NVRTC): with CAVE_JIT=sync every cave_run and
+cave_render_step below runs the kernels compiled for its rule, checked bit-exact against the
 oracle (every cell, every per-tick statistic, GridInfo), and the launch counter proves that the
-specialised kernel, not the generic one, did the ticks."""
+specialised kernels, not the generic one, did the ticks. Every cave_run case runs twice: with
+two ticks per launch (the default; an odd tick count starts with one single-tick launch) and with
+CAVE_TICK2=0 (one tick per launch)."""
 import os
 
 import numpy as np
@@ -11,6 +13,16 @@ import cave_b200 as cb
 import oracle as O
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(params=["pairs", "single"], autouse=True)
+def tick2(request, monkeypatch):
+    monkeypatch.setenv("CAVE_TICK2", "1" if request.param == "pairs" else "0")
+    return request.param == "pairs"
+
+
+def expected_launches(nticks, pairs):
+    return (nticks & 1) + nticks // 2 if pairs and nticks >= 2 else nticks
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -39,19 +51,19 @@ def run_and_check(ctx, X, Y, Z, params_np, init, nticks, max_ticks=10 ** 6):
     p = cb.SimParams(*[int(v) for v in params_np])
     cells, expect = init, []
     for _ in range(nticks):
-        cells, snap = O.step_fast(X, Y, Z, params_np, cells)
-        expect.append(tuple(int(v) for v in snap))
+        cells, st = O.step_stats_fast(X, Y, Z, params_np, cells)
+        expect.append(st.as_tuple())
     _, launches0 = cb.jit_stats()
     with cb.Grid(ctx, X, Y, Z) as g:
         g.upload(init)
         sts, info = g.run(p, nticks, max_ticks)
         got_cells = g.download()
     _, launches1 = cb.jit_stats()
-    assert launches1 - launches0 == nticks, "the ticks did not run on the specialised kernel"
+    pairs = os.environ.get("CAVE_TICK2") != "0"
+    assert launches1 - launches0 == expected_launches(nticks, pairs), "the ticks did not run on the specialised kernels"
     assert np.array_equal(got_cells, cells), "cells differ"
     for t in range(nticks):
-        got = sts[t].as_tuple()
-        assert got[:len(expect[t])] == expect[t], f"statistics differ at tick {t + 1}"
+        assert sts[t].as_tuple() == expect[t], f"statistics differ at tick {t + 1}"
     return info
 
 
@@ -89,6 +101,27 @@ def test_tilings(ctx, dims):
     X, Y, Z = dims
     rng = np.random.default_rng(X + Y + Z)
     run_and_check(ctx, X, Y, Z, O.make_params(15, 0x7, 0x10, 0x18), random_states(rng, X, Y, Z, 15), 4)
+
+
+@pytest.mark.parametrize("nticks", [1, 2, 3, 4, 5, 7, 8])
+def test_tick_counts(ctx, nticks):
+    """Odd counts start with a single-tick launch, then two ticks per launch."""
+    rng = np.random.default_rng(300 + nticks)
+    X, Y, Z = 96, 61, 40
+    params = O.make_params(3, 0x7, 0x70, 0xF0)  # Moore C=4 B{5,6,7} S{5,6,7,8}: busy every tick
+    info = run_and_check(ctx, X, Y, Z, params, random_states(rng, X, Y, Z, 3), nticks, max_ticks=nticks)
+    want = O.run_sim(X, Y, Z, params, random_states(np.random.default_rng(300 + nticks), X, Y, Z, 3), nticks,
+                     fast=True)[0]
+    assert info.as_tuple() == want.as_tuple()
+
+
+@pytest.mark.parametrize("dims", [(32, 1, 1), (33, 2, 3), (64, 3, 5), (100, 5, 2), (257, 130, 9), (512, 200, 33),
+                                  (96, 300, 7), (31, 64, 64)])
+def test_pair_tilings(ctx, dims):
+    """Grids with fewer rows than a tile, a single plane, one row, partial strips, many y-tiles."""
+    X, Y, Z = dims
+    rng = np.random.default_rng(X * 7 + Y * 3 + Z)
+    run_and_check(ctx, X, Y, Z, O.make_params(5, 0x3, 0x18, 0x3C), random_states(rng, X, Y, Z, 5), 6)
 
 
 def test_prepare_then_async(ctx):
