@@ -86,7 +86,7 @@ class SearchConfig(ctypes.Structure):
 class SearchSummary(ctypes.Structure):
     _fields_ = [("sims", u64), ("viable", u64), ("possible", u64), ("unviable", u64), ("ticks", u64),
                 ("cellUpdates", u64), ("chunks", u32), ("uniqueRules", u32), ("deviceSeconds", ctypes.c_double),
-                ("wallSeconds", ctypes.c_double)]
+                ("wallSeconds", ctypes.c_double), ("stopped", u32), ("pad", u32)]
 
 
 def search_config(grid=49, spawn=11, spawn_mode="filled", density=0.5, neighborhood="F", min_cs=3, max_cs=10,
@@ -222,6 +222,7 @@ _SIGS = {
     "cave_render_step": (i32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, u32, u32, u32, P(SimParams), u32,
                                ctypes.c_void_p]),
     "cave_search_run": (i32, [ctypes.c_void_p, P(SearchConfig), u32, u64, P(SearchSummary)]),
+    "cave_search_stop": (i32, [ctypes.c_void_p]),
     "cave_rule_string_to_bitmask": (u64, [ctypes.c_char_p]),
     "cave_bitmask_to_rule_string": (u64, [u64, ctypes.c_char_p, u64]),
 }
@@ -477,6 +478,11 @@ def search_run(ctx: Context, config: SearchConfig, plain=False, sim_limit=0) -> 
     ctx.check(lib().cave_search_run(ctx.h, ctypes.byref(config), 1 if plain else 0, sim_limit, ctypes.byref(s)),
               "cave_search_run")
     return s
+
+
+def search_stop(ctx: Context):
+    """Asks the search_run in progress on ctx (in another thread) to stop after its current wave."""
+    ctx.check(lib().cave_search_stop(ctx.h), "cave_search_stop")
 
 
 def manager_update(snapshot: GridSnapshot, info: GridInfo, perms: SimParams, max_permutation, survival_end,

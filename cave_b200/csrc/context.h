@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <map>
 #include <mutex>
@@ -46,6 +47,7 @@ struct cave_ctx {
     int sm_count = 148;
     int smem_optin = 227 * 1024;  // largest shared memory one CTA may opt in to
     uint32_t last_run_kind = 0;   // tick kernels of the last cave_run (0 generic, 1 specialised, 2 two-tick)
+    std::atomic<bool> search_stop{false};  // set by cave_search_stop (any thread), read between waves
     std::string last_error;
     std::mutex mu;  // guards last_error
     bool timing = false;

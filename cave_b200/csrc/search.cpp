@@ -9,8 +9,10 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <filesystem>
+#include <functional>
 #include <fstream>
 #include <map>
 #include <sstream>
@@ -216,72 +218,156 @@ static bool write_aggregate(const std::string& path, const std::map<AggKey, AggS
     return out.good();
 }
 
+// ---------------------------------------------------------------- output
+// Per-chunk JSONL output, appended and flushed as results arrive (searchSystem.cpp:959-978:
+// one line per finished rule, flushed at once), so that a sweep that is stopped or dies keeps
+// every result written so far. A chunk's three files are created (truncated) when its first
+// results arrive, and reopened for appending by later waves.
+struct ChunkWriter {
+    const Sweep& s;
+    std::vector<char> started;
+    explicit ChunkWriter(const Sweep& sw) : s(sw), started(sw.chunks.size(), 0) {}
+    cave_status write(cave_ctx* ctx, size_t ci, const std::vector<Outcome>& outs) {
+        if (s.folder.empty()) return CAVE_OK;
+        const std::string p = s.folder + chunk_prefix(s, s.chunks[ci]);
+        const char* names[3] = {"_viable.jsonl", "_possible.jsonl", "_unviable.jsonl"};
+        std::ofstream f[3];
+        for (int k = 0; k < 3; k++) {
+            f[k].open(p + names[k], std::ios::out | (started[ci] ? std::ios::app : std::ios::trunc));
+            if (!f[k].is_open()) return set_error(ctx, CAVE_ERR_IO, "cannot write " + p + names[k]);
+        }
+        started[ci] = 1;
+        for (const Outcome& o : outs) f[o.category] << result_line(o) << '\n';
+        for (auto& ff : f) {
+            ff.flush();
+            if (!ff.good()) return set_error(ctx, CAVE_ERR_IO, "JSONL write failed: " + p);
+        }
+        return CAVE_OK;
+    }
+};
+
+// Results of one chunk as they arrive (the chunk's index and its outcomes in rule order).
+using ResultSink = std::function<cave_status(size_t chunk, const std::vector<Outcome>& outs)>;
+
+// Simulations per batched wave: results are written out after each wave, and a stop request
+// is honoured between waves. CAVE_SEARCH_WAVE_SIMS overrides the size.
+static uint64_t wave_sims() {
+    const char* v = std::getenv("CAVE_SEARCH_WAVE_SIMS");
+    const long long n = v ? std::atoll(v) : 0;
+    return n > 0 ? (uint64_t)n : (1ull << 20);
+}
+
+static bool stop_requested(cave_ctx* ctx) { return ctx->search_stop.load(std::memory_order_acquire); }
+
 // ---------------------------------------------------------------- batched execution
-static cave_status run_batched(cave_ctx* ctx, const cave_search_config& c, const Sweep& s,
-                               std::vector<std::vector<Outcome>>& per_chunk, uint64_t limit, double& dev_s,
-                               uint64_t& nsims) {
-    cave_batch* b = nullptr;
-    cave_status rc = cave_batch_create(ctx, &b);
-    if (rc) return rc;
-    struct Guard {
-        cave_batch* b;
-        ~Guard() { cave_batch_destroy(b); }
-    } guard{b};
-    // K-index tables, one per grid config
-    std::vector<uint32_t> table_ix(s.configs.size(), 0);
-    if (c.maxRuleBits > 0)
-        for (size_t i = 0; i < s.configs.size(); i++) {
-            rc = cave_batch_add_table(b, s.configs[i].valid.data(), (uint32_t)s.configs[i].valid.size(), &table_ix[i]);
-            if (rc) return rc;
-        }
-    std::vector<cave_sim_desc> descs;
-    std::vector<std::pair<uint32_t, uint32_t>> owner;  // (chunk, position)
-    for (uint32_t ci = 0; ci < s.chunks.size(); ci++) {
+// The sweep's simulations in chunk order (birth index fastest within a slot, as the reference
+// walks them), run in waves of up to wave_sims() simulations: one batch per wave, holding the
+// initial grids and K-index tables of the chunks the wave touches.
+static cave_status run_batched(cave_ctx* ctx, const cave_search_config& c, const Sweep& s, const ResultSink& sink,
+                               uint64_t limit, double& dev_s, uint64_t& nsims, bool& stopped) {
+    struct Piece {
+        uint32_t chunk, gi;
+        uint64_t sv, bi;  // first simulation of the piece
+    };
+    dev_s = 0;
+    nsims = 0;
+    stopped = false;
+    const uint64_t per_wave = wave_sims();
+    // simulations of chunk ci, slot gi, in order
+    auto chunk_sims = [&](uint32_t ci, std::vector<std::pair<uint32_t, std::pair<uint64_t, uint64_t>>>& out) {
         const Chunk& ch = s.chunks[ci];
-        // initial cells per maxCellState (searchSystem.cpp:219-306): one grid per distinct maxCS
-        std::map<uint32_t, uint32_t> init_ix;
-        const bool random = ch.spawnRegionShapeId == 0;
-        const uint64_t thr = random ? threshold_from_index(ch.densityIndex) : (1ull << 32);
-        for (size_t gi = 0; gi < s.configs.size(); gi++) {
-            const uint32_t m = s.configs[gi].maxCellState;
-            if (init_ix.count(m)) continue;
-            uint32_t ix = 0;
-            rc = cave_batch_add_init_seeded(b, ch.X, ch.Y, ch.Z, ch.spawnX, ch.spawnY, ch.spawnZ, thr, ch.seed, m, &ix);
-            if (rc) return rc;
-            init_ix[m] = ix;
-        }
         for (uint32_t gi = 0; gi < s.configs.size(); gi++) {
-            const GridConfig& g = s.configs[gi];
             uint64_t lo, hi;
-            survival_range(g, ch, lo, hi);
+            survival_range(s.configs[gi], ch, lo, hi);
             for (uint64_t sv = lo; sv <= hi; sv++)
-                for (uint64_t bi = 1; bi <= g.maxPermutation; bi++) {  // birth index fastest
-                    if (limit && descs.size() >= limit) break;
-                    cave_sim_desc d{};
-                    d.params.birthAndMaxCellStateRules = ((uint64_t)((g.maxCellState - 1) & 0xF) << 60) | bi;
-                    d.params.survivalAndNeighborhoodRules = ((uint64_t)(g.flags & 0xF) << 60) | sv;
-                    d.params.shapeAndGridConfiguration = 0;
-                    d.init = init_ix[g.maxCellState];
-                    d.maxTicks = c.maxTicks;
-                    d.validTable = table_ix[gi];
-                    d.tag = (uint32_t)descs.size();
-                    owner.emplace_back(ci, gi);
-                    descs.push_back(d);
+                for (uint64_t bi = 1; bi <= s.configs[gi].maxPermutation; bi++) out.push_back({gi, {sv, bi}});
+        }
+    };
+    std::vector<std::pair<uint32_t, std::pair<uint64_t, uint64_t>>> sims_of;  // (slot, (survival, birth))
+    uint32_t ci = 0;
+    size_t pos = 0;  // next simulation of chunk ci
+    bool loaded = false;
+    while (ci < s.chunks.size() && !(limit && nsims >= limit)) {
+        if (stop_requested(ctx)) {
+            stopped = true;
+            break;
+        }
+        // ---- one wave
+        cave_batch* b = nullptr;
+        cave_status rc = cave_batch_create(ctx, &b);
+        if (rc) return rc;
+        struct Guard {
+            cave_batch* b;
+            ~Guard() { cave_batch_destroy(b); }
+        } guard{b};
+        std::vector<uint32_t> table_ix(s.configs.size(), 0);
+        if (c.maxRuleBits > 0)
+            for (size_t i = 0; i < s.configs.size(); i++) {
+                rc = cave_batch_add_table(b, s.configs[i].valid.data(), (uint32_t)s.configs[i].valid.size(),
+                                          &table_ix[i]);
+                if (rc) return rc;
+            }
+        std::vector<cave_sim_desc> descs;
+        std::vector<uint32_t> owner;  // chunk of each simulation
+        while (ci < s.chunks.size() && descs.size() < per_wave && !(limit && nsims + descs.size() >= limit)) {
+            if (!loaded) {
+                sims_of.clear();
+                chunk_sims(ci, sims_of);
+                pos = 0;
+                loaded = true;
+            }
+            const Chunk& ch = s.chunks[ci];
+            // initial cells per maxCellState (searchSystem.cpp:219-306): one grid per distinct maxCS
+            std::map<uint32_t, uint32_t> init_ix;
+            const bool random = ch.spawnRegionShapeId == 0;
+            const uint64_t thr = random ? threshold_from_index(ch.densityIndex) : (1ull << 32);
+            for (; pos < sims_of.size() && descs.size() < per_wave && !(limit && nsims + descs.size() >= limit); pos++) {
+                const uint32_t gi = sims_of[pos].first;
+                const GridConfig& g = s.configs[gi];
+                auto it = init_ix.find(g.maxCellState);
+                if (it == init_ix.end()) {
+                    uint32_t ix = 0;
+                    rc = cave_batch_add_init_seeded(b, ch.X, ch.Y, ch.Z, ch.spawnX, ch.spawnY, ch.spawnZ, thr, ch.seed,
+                                                    g.maxCellState, &ix);
+                    if (rc) return rc;
+                    it = init_ix.emplace(g.maxCellState, ix).first;
                 }
+                cave_sim_desc d{};
+                d.params.birthAndMaxCellStateRules = ((uint64_t)((g.maxCellState - 1) & 0xF) << 60) | sims_of[pos].second.second;
+                d.params.survivalAndNeighborhoodRules = ((uint64_t)(g.flags & 0xF) << 60) | sims_of[pos].second.first;
+                d.params.shapeAndGridConfiguration = 0;
+                d.init = it->second;
+                d.maxTicks = c.maxTicks;
+                d.validTable = table_ix[gi];
+                d.tag = (uint32_t)descs.size();
+                owner.push_back(ci);
+                descs.push_back(d);
+            }
+            if (pos >= sims_of.size()) {
+                ci++;
+                loaded = false;
+            }
+        }
+        if (descs.empty()) break;
+        rc = cave_batch_add_sims(b, descs.data(), descs.size(), c.maxRuleBits);
+        if (rc) return rc;
+        rc = cave_batch_launch(b);
+        if (rc) return rc;
+        std::vector<cave_sim_result> res(descs.size());
+        rc = cave_batch_results(b, res.data(), res.size());
+        if (rc) return rc;
+        dev_s += ctx->last_timing.tick_ms / 1e3;  // the wave's kernels, resident and tiled
+        nsims += descs.size();
+        // hand each chunk's results over in order
+        size_t i = 0;
+        while (i < res.size()) {
+            const uint32_t chunk = owner[i];
+            std::vector<Outcome> outs;
+            for (; i < res.size() && owner[i] == chunk; i++) outs.push_back(Outcome{res[i].params, res[i].info, res[i].category});
+            rc = sink(chunk, outs);
+            if (rc) return rc;
         }
     }
-    rc = cave_batch_add_sims(b, descs.data(), descs.size(), c.maxRuleBits);
-    if (rc) return rc;
-    rc = cave_batch_launch(b);
-    if (rc) return rc;
-    std::vector<cave_sim_result> res(descs.size());
-    rc = cave_batch_results(b, res.data(), res.size());
-    if (rc) return rc;
-    dev_s = ctx->last_timing.tick_ms / 1e3;  // the batch's kernels, resident and tiled
-    nsims = descs.size();
-    per_chunk.assign(s.chunks.size(), {});
-    for (size_t i = 0; i < res.size(); i++)
-        per_chunk[owner[i].first].push_back(Outcome{res[i].params, res[i].info, res[i].category});
     return CAVE_OK;
 }
 
@@ -289,18 +375,22 @@ static cave_status run_batched(cave_ctx* ctx, const cave_search_config& c, const
 // SearchSystem's loop (searchSystem.cpp:480-713): per tick, reset finished slots from their
 // initial cells, launch the step (with the fused manager) once per slot, fence, read the copy
 // buffers and record finished rules.
-static cave_status run_plain(cave_ctx* ctx, const cave_search_config& c, const Sweep& s,
-                             std::vector<std::vector<Outcome>>& per_chunk, uint64_t limit, double& dev_s,
-                             uint64_t& nsims) {
-    per_chunk.assign(s.chunks.size(), {});
+static cave_status run_plain(cave_ctx* ctx, const cave_search_config& c, const Sweep& s, const ResultSink& sink,
+                             uint64_t limit, double& dev_s, uint64_t& nsims, bool& stopped) {
     nsims = 0;
+    stopped = false;
     double dev_ms = 0;
     cudaEvent_t e0, e1;
     CAVE_CUDA(ctx, cudaEventCreate(&e0));
     CAVE_CUDA(ctx, cudaEventCreate(&e1));
     for (uint32_t ci = 0; ci < s.chunks.size() && !(limit && nsims >= limit); ci++) {
+        if (stop_requested(ctx)) {
+            stopped = true;
+            break;
+        }
         const Chunk& ch = s.chunks[ci];
         const uint32_t nslot = (uint32_t)s.configs.size();
+        std::vector<Outcome> outs;  // this chunk's results, handed over when it completes
         const uint64_t words = cave_grid_words(ch.X, ch.Y, ch.Z);
         // device buffers: per slot cur/next/initial cells, the slot records, K-index tables
         uint32_t* cells = nullptr;
@@ -407,13 +497,18 @@ static cave_status run_plain(cave_ctx* ctx, const cave_search_config& c, const S
                 o.info = info;
                 const uint64_t mcs = ((pm.birthAndMaxCellStateRules >> 60) & 0xF) + 1;
                 o.category = info.status == 2 ? 0u : ((uint64_t)info.numberOfSimulationTicksSurvived > mcs + 1 ? 1u : 2u);
-                per_chunk[ci].push_back(o);
+                outs.push_back(o);
                 nsims++;
             }
         }
         cudaFree(cells);
         cudaFree(slots);
         cudaFree(tables);
+        if (cave_status rc = sink(ci, outs); rc != CAVE_OK) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return rc;
+        }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -434,53 +529,69 @@ cave_status cave_search_run(cave_ctx* ctx, const cave_search_config* config, uin
     if (c.minMaxCellState < 1 || c.maxMaxCellState > 16 || c.minMaxCellState > c.maxMaxCellState || c.maxTicks == 0)
         return set_error(ctx, CAVE_ERR_INVALID_ARG, "maxCellState range must lie in 1..16 and ticks must be > 0");
     const auto t0 = std::chrono::steady_clock::now();
+    ctx->search_stop.store(false, std::memory_order_release);  // a stop applies to the run in progress
     CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
     Sweep s = expand(c);
     for (const Chunk& ch : s.chunks)
         if (ch.X == 0 || ch.Y == 0 || ch.Z == 0) return set_error(ctx, CAVE_ERR_INVALID_ARG, "grid extents must be > 0");
-    std::vector<std::vector<Outcome>> per_chunk;
-    double dev_s = 0;
-    uint64_t nsims = 0;
-    cave_status rc = mode == 0 ? run_batched(ctx, c, s, per_chunk, simLimit, dev_s, nsims)
-                               : run_plain(ctx, c, s, per_chunk, simLimit, dev_s, nsims);
-    if (rc) return rc;
-    cave_search_summary sum{};
-    std::map<AggKey, AggStats> agg;
     if (!s.folder.empty()) {
         std::error_code ec;
         std::filesystem::create_directories(s.folder, ec);
-        if (ec) return set_error(ctx, CAVE_ERR_IO, "cannot create " + s.folder);
+        if (ec) return set_error(ctx, CAVE_ERR_IO, "cannot create " + s.folder + ": " + ec.message());
     }
-    for (size_t ci = 0; ci < s.chunks.size(); ci++) {
+    cave_search_summary sum{};
+    std::map<AggKey, AggStats> agg;
+    ChunkWriter writer(s);
+    std::vector<char> chunk_done(s.chunks.size(), 0);
+    // every chunk's results: into the summary and the aggregate (ruleAggregator.h:69-90), then
+    // appended to its files
+    const ResultSink sink = [&](size_t ci, const std::vector<Outcome>& outs) -> cave_status {
         const Chunk& ch = s.chunks[ci];
-        std::ofstream f[3];
-        if (!s.folder.empty()) {
-            const std::string p = s.folder + chunk_prefix(s, ch);
-            const char* names[3] = {"_viable.jsonl", "_possible.jsonl", "_unviable.jsonl"};
-            for (int k = 0; k < 3; k++) {
-                f[k].open(p + names[k], std::ios::out | std::ios::trunc);
-                if (!f[k].is_open()) return set_error(ctx, CAVE_ERR_IO, "cannot write " + p + names[k]);
-            }
-        }
-        for (const Outcome& o : per_chunk[ci]) {
+        for (const Outcome& o : outs) {
             sum.sims++;
             (o.category == 0 ? sum.viable : o.category == 1 ? sum.possible : sum.unviable)++;
             sum.ticks += o.info.numberOfSimulationTicksSurvived;
             sum.cellUpdates += (uint64_t)o.info.numberOfSimulationTicksSurvived * ch.X * ch.Y * ch.Z;
             aggregate(agg, o);
-            if (!s.folder.empty()) f[o.category] << result_line(o) << '\n';
         }
-        for (auto& ff : f)
-            if (ff.is_open() && !ff.good()) return set_error(ctx, CAVE_ERR_IO, "JSONL write failed");
+        chunk_done[ci] = 1;
+        return writer.write(ctx, ci, outs);
+    };
+    double dev_s = 0;
+    uint64_t nsims = 0;
+    bool stopped = false;
+    cave_status rc = mode == 0 ? run_batched(ctx, c, s, sink, simLimit, dev_s, nsims, stopped)
+                               : run_plain(ctx, c, s, sink, simLimit, dev_s, nsims, stopped);
+    if (rc) return rc;
+    if (!s.folder.empty()) {
+        if (!stopped) {
+            // chunks without any result (an empty sweep range) still get their three files
+            for (size_t ci = 0; ci < s.chunks.size(); ci++)
+                if (!chunk_done[ci] && !simLimit) {
+                    rc = writer.write(ctx, ci, {});
+                    if (rc) return rc;
+                }
+            if (!write_aggregate(s.folder + s.prefixBase + "_aggregate.jsonl", agg))
+                return set_error(ctx, CAVE_ERR_IO, "aggregate JSONL write failed");
+        } else if (!agg.empty()) {
+            // searchMode.cpp:437-449: a stopped sweep writes what it has as a partial aggregate
+            if (!write_aggregate(s.folder + s.prefixBase + "_aggregate_partial.jsonl", agg))
+                return set_error(ctx, CAVE_ERR_IO, "partial aggregate JSONL write failed");
+        }
     }
-    if (!s.folder.empty() && !write_aggregate(s.folder + s.prefixBase + "_aggregate.jsonl", agg))
-        return set_error(ctx, CAVE_ERR_IO, "aggregate JSONL write failed");
     sum.chunks = (uint32_t)s.chunks.size();
     sum.uniqueRules = (uint32_t)agg.size();
     sum.deviceSeconds = dev_s;
     sum.wallSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    sum.stopped = stopped ? 1u : 0u;
     (void)nsims;
     if (summary) *summary = sum;
+    return CAVE_OK;
+}
+
+cave_status cave_search_stop(cave_ctx* ctx) {
+    if (!ctx) return CAVE_ERR_INVALID_ARG;
+    ctx->search_stop.store(true, std::memory_order_release);
     return CAVE_OK;
 }
 

@@ -438,20 +438,33 @@ typedef struct {
     uint32_t uniqueRules;    /* entries of the aggregate                              */
     double deviceSeconds;    /* device time of the simulation work (CUDA events)      */
     double wallSeconds;      /* whole call                                            */
+    uint32_t stopped;        /* 1: cave_search_stop ended the sweep early             */
+    uint32_t pad;
 } cave_search_summary;
 
 /* Runs a whole sweep as SearchMode::OnFrame does (searchMode.cpp:49-218 expansion,
  * :252-459 run, :1030-1054 files and aggregation) and writes, when outputFolder is set,
  * <out>cube/<prefix>_c<n>_g<X>x<Y>x<Z>_d<d>_s<s>_gpu0_{viable,possible,unviable}.jsonl per chunk
  * (searchSystem.cpp:959-978 line format, keys sorted) and <out>cube/<prefix>_aggregate.jsonl
- * (ruleAggregator.h:105-134). mode 0 runs every simulation to completion on the device in
- * persistent batched launches; mode 1 is the plain path, SearchSystem's own loop -- one
- * launch per slot per tick and a host fence per tick (searchSystem.cpp:480-713).
+ * (ruleAggregator.h:105-134). mode 0 runs the simulations on the device in persistent batched
+ * launches, in waves of up to 2^20 simulations (CAVE_SEARCH_WAVE_SIMS overrides); mode 1 is the
+ * plain path, SearchSystem's own loop -- one launch per slot per tick and a host fence per tick
+ * (searchSystem.cpp:480-713), a chunk at a time. Results are appended to their chunk's files and
+ * flushed after every wave (mode 0) or chunk (mode 1), as the reference appends and flushes each
+ * line (searchSystem.cpp:974-977), so a sweep that is stopped or dies keeps what it wrote.
  * simLimit > 0 stops after that many simulations (for sampling the plain path). Lines within
  * a file are in rule order (slot, survival, birth); the reference writes them in completion
- * order, which depends on scheduling. */
+ * order, which depends on scheduling. A folder that cannot be created or a file that cannot be
+ * written gives CAVE_ERR_IO. */
 cave_status cave_search_run(cave_ctx* ctx, const cave_search_config* config, uint32_t mode, uint64_t simLimit,
                             cave_search_summary* summary);
+/* Asks the cave_search_run in progress on ctx to stop (the reference's stop request,
+ * searchMode.cpp:437-449): it finishes the wave or chunk on the device, writes its results, then
+ * writes <out>cube/<prefix>_aggregate_partial.jsonl (when any rule finished) instead of the
+ * aggregate and returns CAVE_OK with summary->stopped = 1. Safe to call from any host thread while
+ * the run is in progress (the one exception to one thread per context); a request made when no
+ * run is in progress is dropped by the next run's start. */
+cave_status cave_search_stop(cave_ctx* ctx);
 
 /* Reference rule-string helpers (guiSystem.cpp:92-163): "3,5-7" <-> bitmask (bit n-1 = n). */
 uint64_t cave_rule_string_to_bitmask(const char* rule);

@@ -258,6 +258,37 @@ def classify(info: GridInfo, max_cell_state: int) -> int:
     return lib().oracle_classify(ctypes.byref(info), max_cell_state)
 
 
+def aggregate_lines(results, shape_id=0):
+    """RuleAggregator restated (src/common/ruleAggregator.h:69-90 Record, :105-135 WriteJsonl):
+    results = iterable of (birth field, survival field, ticks survived, category 0/1/2) with the
+    rule fields in bitmask form. Rule identity = (birth mask, survival mask, maxCellState,
+    neighbourhood flags, shape id); per rule: runs per category, min / max / average ticks and the
+    viable fraction, the two averages computed in float32 and printed like a C++ ostream float
+    (six significant digits, %g). Returns {rule key: JSONL line} in the reference's key order."""
+    import numpy as _np
+
+    stats = {}
+    for birth, survival, ticks, cat in results:
+        birth, survival = int(birth), int(survival)
+        key = (birth & PERM_MASK, survival & PERM_MASK, ((birth >> 60) & 0xF) + 1, survival >> 60, shape_id)
+        st = stats.setdefault(key, [0, 0, 0, 0, 0, 0xFFFFFFFF, 0])
+        st[0] += 1
+        st[1 + int(cat)] += 1
+        st[4] = max(st[4], int(ticks))
+        st[5] = min(st[5], int(ticks))
+        st[6] += int(ticks)
+    out = {}
+    for key, (total, viable, possible, unviable, mx, mn, sm) in stats.items():
+        avg = _np.float32(sm) / _np.float32(total) if total else _np.float32(0)
+        rate = _np.float32(viable) / _np.float32(total) if total else _np.float32(0)
+        out[key] = ("{\"birth\":%d,\"survival\":%d,\"maxCellState\":%d,\"neighborhoodFlags\":%d,\"shapeId\":%d,"
+                    "\"totalRuns\":%d,\"viableRuns\":%d,\"possibleRuns\":%d,\"unviableRuns\":%d,"
+                    "\"viabilityRate\":%s,\"minTicksSurvived\":%d,\"maxTicksSurvived\":%d,\"avgTicksSurvived\":%s}"
+                    % (key + (total, viable, possible, unviable, "%g" % float(rate), 0 if mn == 0xFFFFFFFF else mn, mx,
+                              "%g" % float(avg))))
+    return out
+
+
 def run_slot(X, Y, Z, start_birth_field, start_survival_field, max_permutation, survival_end, initial,
              max_ticks, valid=None, max_rule_bits=0, fast=True, cap=1 << 16):
     initial = np.ascontiguousarray(initial, dtype=np.uint32)

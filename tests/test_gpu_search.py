@@ -156,3 +156,93 @@ def test_reference_benchmark_sweep_vs_fixture(ctx, G):
     assert (int((cats == 0).sum()), int((cats == 1).sum()), int((cats == 2).sum())) == (
         fx["viable"], fx["possible"], fx["unviable"])
     assert hashlib.sha256(arr.tobytes()).hexdigest() == fx["gridinfo_sha256"]
+
+
+def oracle_chunk_results(G, flags_list, cs_range, K, T, spawn, seed=0, random=False, density_index=0):
+    """(birth field, survival field, ticks, category) of every rule of one chunk (oracle_run_slot)."""
+    out = []
+    thr = O.threshold_from_index(density_index) if random else 1 << 32
+    for mcs in cs_range:
+        init = O.seed(G, G, G, spawn=(spawn,) * 3, random=random, threshold=thr, run_seed=seed, max_cell_state=mcs)
+        for flags in flags_list:
+            n = NB[flags & 7]
+            vb = O.valid_bitmasks(n, K) if K else None
+            maxp = len(vb) if K else (1 << n) - 1
+            for r in O.run_slot(G, G, G, ((mcs - 1) << 60) | 1, (flags << 60) | 1, maxp, maxp, init, T, valid=vb,
+                                max_rule_bits=K, fast=True):
+                out.append((r.birthAndMaxCellStateRules, r.survivalAndNeighborhoodRules, r.info.ticks, r.category))
+    return out
+
+
+@pytest.mark.parametrize("plain", [False, True])
+def test_aggregate_values_match_oracle(ctx, tmp_path, plain):
+    """Every aggregate line -- runs per category, viabilityRate, min / max / avg ticks -- equals the
+    oracle's RuleAggregator restatement over the oracle pipeline's results, across seeds and
+    densities (each rule aggregated over four chunks)."""
+    G, T = 8, 12
+    out = str(tmp_path) + "/"
+    cfg = cb.search_config(grid=G, spawn=6, spawn_mode="random", neighborhood="F", min_cs=2, max_cs=4, ticks=T,
+                           seed_runs=2, density_sweep=(0.25, 0.5, 0.25), output=out)
+    s = cb.search_run(ctx, cfg, plain=plain)
+    results = []
+    for di in (3, 7):
+        for seed in range(2):
+            results += oracle_chunk_results(G, [1], (2, 3, 4), 0, T, 6, seed=seed, random=True, density_index=di)
+    want = O.aggregate_lines(results)
+    got = open(os.path.join(out, "cube", f"cs2-4_F_t{T}_aggregate.jsonl")).read().splitlines()
+    assert len(got) == len(want) == s.uniqueRules == 3 * 63 * 63
+    assert sorted(got) == sorted(want.values())
+    assert s.sims == len(results) and not s.stopped
+
+
+def test_stop_keeps_written_results_and_writes_partial_aggregate(ctx, tmp_path, monkeypatch):
+    """A stop request mid-sweep (searchMode.cpp:437-449): results written so far stay in their
+    files (each line flushed as its wave finished), the aggregate of what ran goes to
+    _aggregate_partial.jsonl, and no full aggregate is written."""
+    import threading
+    import time
+
+    monkeypatch.setenv("CAVE_SEARCH_WAVE_SIMS", "256")
+    G, T, K = 9, 8, 2
+    out = str(tmp_path) + "/"
+    cfg = cb.search_config(grid=G, spawn=5, spawn_mode="filled", neighborhood="FE", min_cs=2, max_cs=3, ticks=T,
+                           max_rule_bits=K, seed_runs=3, output=out)
+    box = {}
+    th = threading.Thread(target=lambda: box.setdefault("s", cb.search_run(ctx, cfg)))
+    th.start()
+    first = os.path.join(out, "cube", f"cs2-3_FE_t{T}_b{K}_c1_g{G}x{G}x{G}_d7_s0_gpu0_unviable.jsonl")
+    t0 = time.time()
+    while not (os.path.exists(first) and os.path.getsize(first) > 0) and th.is_alive() and time.time() - t0 < 120:
+        time.sleep(0.001)
+    cb.search_stop(ctx)
+    th.join(300)
+    s = box["s"]
+    assert s.stopped == 1
+    total = (21 * 21 + 78 * 78 + 171 * 171) * 2 * 3
+    assert 0 < s.sims < total
+    cube = os.path.join(out, "cube")
+    assert not os.path.exists(os.path.join(cube, f"cs2-3_FE_t{T}_b{K}_aggregate.jsonl"))
+    partial = open(os.path.join(cube, f"cs2-3_FE_t{T}_b{K}_aggregate_partial.jsonl")).read().splitlines()
+    # every written line is one of the oracle's, and the partial aggregate is the aggregate of them
+    written = []
+    expect = oracle_chunk(G, [1, 2, 3], (2, 3), K, T, 5)  # the spawn is filled: every seed has the same cells
+    for f in sorted(glob.glob(os.path.join(cube, "*.jsonl"))):
+        if "aggregate" in f:
+            continue
+        cat = 0 if f.endswith("_viable.jsonl") else 1 if f.endswith("_possible.jsonl") else 2
+        for line in open(f).read().splitlines():
+            assert line in expect[cat], f
+            d = json.loads(line)
+            written.append((d["birthAndMaxCellStateRules"], d["survivalAndNeighborhoodRules"], d["ticksSurvived"], cat))
+    assert len(written) == s.sims
+    assert sorted(partial) == sorted(O.aggregate_lines(written).values())
+
+
+def test_unwritable_output_folder_is_an_io_error(ctx, tmp_path):
+    blocker = tmp_path / "not_a_folder"
+    blocker.write_text("x")
+    cfg = cb.search_config(grid=7, spawn=5, neighborhood="F", min_cs=2, max_cs=2, ticks=4,
+                           output=str(blocker) + "/out/")
+    with pytest.raises(cb.CaveError) as e:
+        cb.search_run(ctx, cfg)
+    assert e.value.code == cb.ERR_IO

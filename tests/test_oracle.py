@@ -250,3 +250,20 @@ def test_slot_pipeline_equals_independent_rules():
         info, _, _ = O.run_sim(G, G, G, p, init, 10)
         assert info.as_tuple() == r.info.as_tuple()
         assert O.classify(info, 2) == r.category
+
+
+def test_aggregate_lines_known_answer():
+    """RuleAggregator (ruleAggregator.h:69-90, :105-135): rule identity, per-category runs, min /
+    max ticks, float32 averages printed with six significant digits in the reference's key
+    order."""
+    runs = [((2 << 60) | 5, (3 << 60) | 9, 20, 0), ((2 << 60) | 5, (3 << 60) | 9, 7, 2),
+            ((2 << 60) | 5, (3 << 60) | 9, 20, 0), ((0 << 60) | 5, (3 << 60) | 9, 4, 1)]
+    got = O.aggregate_lines(runs)
+    assert got[(5, 9, 3, 3, 0)] == ('{"birth":5,"survival":9,"maxCellState":3,"neighborhoodFlags":3,"shapeId":0,'
+                                    '"totalRuns":3,"viableRuns":2,"possibleRuns":0,"unviableRuns":1,'
+                                    '"viabilityRate":0.666667,"minTicksSurvived":7,"maxTicksSurvived":20,'
+                                    '"avgTicksSurvived":15.6667}')
+    assert got[(5, 9, 1, 3, 0)] == ('{"birth":5,"survival":9,"maxCellState":1,"neighborhoodFlags":3,"shapeId":0,'
+                                    '"totalRuns":1,"viableRuns":0,"possibleRuns":1,"unviableRuns":0,'
+                                    '"viabilityRate":0,"minTicksSurvived":4,"maxTicksSurvived":4,'
+                                    '"avgTicksSurvived":4}')
