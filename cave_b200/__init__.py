@@ -215,6 +215,7 @@ _SIGS = {
     "cave_server_submit": (i32, [ctypes.c_void_p, ctypes.c_void_p, u64, P(u64)]),
     "cave_server_poll": (i32, [ctypes.c_void_p, P(u64), u64, P(u64)]),
     "cave_server_wait": (i32, [ctypes.c_void_p, u64, ctypes.c_double]),
+    "cave_server_cancel": (i32, [ctypes.c_void_p, u64]),
     "cave_server_fetch": (i32, [ctypes.c_void_p, u64, ctypes.c_void_p, u64, P(ctypes.c_double)]),
     "cave_server_get_stats": (i32, [ctypes.c_void_p, P(ServerStats)]),
     "cave_render_buffer_elements": (u64, [u32, u32, u32]),
@@ -635,6 +636,11 @@ class Server:
             return False
         self.ctx.check(rc, "cave_server_wait")
         return True
+
+    def cancel(self, rid):
+        """Cancels a request: queued simulations leave the queue, running ones finish unreported."""
+        self.ctx.check(lib().cave_server_cancel(self.h, rid), "cave_server_cancel")
+        self.sizes.pop(rid, None)
 
     def fetch(self, rid):
         """(results as SIM_RESULT_DTYPE array, latency seconds) of a completed request."""

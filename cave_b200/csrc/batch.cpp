@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -324,6 +325,14 @@ cave_status cave_batch_launch(cave_batch* b) {
         uint32_t threads = 0;
         L.P = resident_geometry(std::get<0>(key), std::get<1>(key), std::get<2>(key), std::get<5>(key), threads);
         L.P.n_sims = (uint32_t)idx.size();
+        // Failure test (CAVE_TEST_WITHHOLD_INIT_COPY): the resident kernel never issues the initial
+        // grid's copy and gives up waiting for it after 1 ms, raising the timeout flag that the
+        // results report as CAVE_ERR_TIMEOUT. Only a batch of exactly one simulation: no copy is
+        // then in flight anywhere when the CTA stops waiting.
+        if (n == 1 && std::getenv("CAVE_TEST_WITHHOLD_INIT_COPY")) {
+            L.P.hold_init = 1;
+            L.P.wait_us = 1000;
+        }
         L.nb = std::get<3>(key);
         L.nt = std::get<4>(key);
         L.threads = threads;

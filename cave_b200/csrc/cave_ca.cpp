@@ -441,11 +441,11 @@ constexpr uint32_t kTuneMinTicks = 100;
 enum RunKind : uint32_t { kRunGeneric = 0, kRunJit = 1, kRunJitPair = 2 };
 
 static uint32_t kind_spt(uint32_t kind) {
-    return kind == kRunGeneric ? 1u : kind == kRunJit ? (uint32_t)kJitRowsPerThread : (uint32_t)kJit2RowsPerThread;
+    return kind == kRunGeneric ? 1u : kind == kRunJit ? (uint32_t)kJitRowsPerThread : tick2_geometry().rows_per_thread;
 }
 static uint32_t kind_halo(uint32_t kind) { return kind == kRunJitPair ? 2u : 1u; }
 static uint32_t kind_max_threads(uint32_t kind) {
-    return kind == kRunGeneric ? 1024u : kind == kRunJit ? (uint32_t)kJitMaxThreads : (uint32_t)kJit2MaxThreads;
+    return kind == kRunGeneric ? 1024u : kind == kRunJit ? (uint32_t)kJitMaxThreads : tick2_geometry().max_threads;
 }
 // Dynamic shared memory the two-tick kernels may take (their static share is a few KB).
 static bool pair_smem_fits(const cave_ctx* ctx, const StreamPlan& p) {
@@ -461,17 +461,18 @@ static bool run_plan(const cave_ctx* ctx, const cave_grid* g, uint32_t rows, uin
     const uint32_t sms = (uint32_t)ctx->sm_count;
     const uint32_t spt = kind_spt(kind), halo = kind_halo(kind), most = kind_max_threads(kind);
     if (kind == kRunGeneric) return plan_stream(0, g->X, g->Y, g->Z, sms * cps, rows, plan, 1);
-    if (!plan_stream(0, g->X, g->Y, g->Z, sms * (cps_given ? cps : 1u), rows, plan, spt, halo)) return false;
+    if (!plan_stream(0, g->X, g->Y, g->Z, sms * (cps_given ? cps : 1u), rows, plan, spt, halo, most)) return false;
     if (kind == kRunJitPair) {
         const uint32_t step = std::max(1u, 32u / plan.SXp) * spt;
         while (!pair_smem_fits(ctx, plan)) {
             if (plan.rows < 2 * halo + 1 + step) return false;
-            if (!plan_stream(0, g->X, g->Y, g->Z, sms * (cps_given ? cps : 1u), plan.rows - step, plan, spt, halo))
+            if (!plan_stream(0, g->X, g->Y, g->Z, sms * (cps_given ? cps : 1u), plan.rows - step, plan, spt, halo,
+                             most))
                 return false;
         }
     }
     if (!cps_given && plan.threads < most)
-        return plan_stream(0, g->X, g->Y, g->Z, sms * (most / plan.threads), plan.rows, plan, spt, halo);
+        return plan_stream(0, g->X, g->Y, g->Z, sms * (most / plan.threads), plan.rows, plan, spt, halo, most);
     return true;
 }
 

@@ -16,7 +16,7 @@ constexpr uint64_t kPermMask = (uint64_t(1) << 60) - 1;  // simulation.h:43
 constexpr uint64_t kWaitLimitNs = 1000000000ull;
 
 // Error flags a kernel may raise in its record (read back by the host).
-enum : uint32_t { kErrNone = 0, kErrWaitTimeout = 1, kErrBadRuleIndex = 2 };
+enum : uint32_t { kErrNone = 0, kErrWaitTimeout = 1, kErrBadRuleIndex = 2, kErrCancelled = 4 };
 
 // Per-grid device record of the plain path. It holds what the reference keeps in the
 // per-slot permutation / snapshot / GridInfo / copy buffers (searchSystem.cpp:202-374).

@@ -252,6 +252,11 @@ cave_status Engine::submit(std::vector<EngineSim>& sims) {
     return CAVE_OK;
 }
 
+void Engine::cancel(uint64_t key_lo, uint64_t key_hi) {
+    std::lock_guard<std::mutex> lock(mu_);
+    cancels_.push_back({key_lo, key_hi});
+}
+
 void Engine::take_results(std::vector<EngineResult>& out) {
     std::lock_guard<std::mutex> lock(mu_);
     out.insert(out.end(), results_.begin(), results_.end());
@@ -583,6 +588,24 @@ cave_status Engine::admit(std::vector<EngineSim>& admitted) {
         while (!incoming_.empty()) {
             pending_.push_back(incoming_.front());
             incoming_.pop_front();
+        }
+        // cancelled simulations leave the queue, reported with the cancelled flag
+        if (!cancels_.empty()) {
+            std::deque<EngineSim> keep;
+            for (EngineSim& s : pending_) {
+                bool drop = false;
+                for (const auto& [lo, hi] : cancels_) drop = drop || (s.key >= lo && s.key < hi);
+                if (!drop) {
+                    keep.push_back(s);
+                    continue;
+                }
+                EngineResult r{};
+                r.key = s.key;
+                r.result.error = kErrCancelled;
+                results_.push_back(r);
+            }
+            pending_.swap(keep);
+            cancels_.clear();
         }
     }
     while (!pending_.empty() && !free_slots_.empty()) {

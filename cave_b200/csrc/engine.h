@@ -125,6 +125,10 @@ public:
     cave_status record_end(cudaEvent_t ev);
     // Moves finished results into out (appends).
     void take_results(std::vector<EngineResult>& out);
+    // Drops the simulations with keys in [key_lo, key_hi) that are not admitted yet; each is
+    // reported by take_results with its result's error set to kErrCancelled. Admitted ones run
+    // to completion. Any thread; applied by the driving thread's next step.
+    void cancel(uint64_t key_lo, uint64_t key_hi);
     EngineStats stats();
     // Device time from the first set-up to the last completed work (CUDA events), ms.
     float device_ms();
@@ -174,6 +178,7 @@ private:
     std::deque<EngineSim> incoming_;
     std::deque<EngineSim> pending_;
     std::vector<EngineResult> results_;
+    std::vector<std::pair<uint64_t, uint64_t>> cancels_;  // key ranges to drop from the queues
     EngineStats stats_;
     cudaEvent_t ev_first_ = nullptr, ev_last_ = nullptr;
     bool first_recorded_ = false;

@@ -179,8 +179,8 @@ std::vector<std::string> options_for(const JitKey& k) {
     std::snprintf(b[3], sizeof b[3], "-DCAVE_JIT_LUT_B=0x%xu", k.lut_b);
     // -default-device: the C header's declarations (host functions) are parsed as device ones
     return {"--gpu-architecture=sm_100a", "-std=c++20", "-default-device", "-lineinfo", b[0], b[1], b[2], b[3],
-            "-DCAVE_TICK2_ROWS=" + std::to_string(kJit2RowsPerThread),
-            "-DCAVE_TICK2_THREADS=" + std::to_string(kJit2MaxThreads)};
+            "-DCAVE_TICK2_ROWS=" + std::to_string(tick2_geometry().rows_per_thread),
+            "-DCAVE_TICK2_THREADS=" + std::to_string(tick2_geometry().max_threads)};
 }
 
 // Compiles the kernel for k (or reads it from the disk cache). No device is touched.
@@ -375,6 +375,22 @@ std::atomic<uint32_t> g_loaded{0};
 std::atomic<uint64_t> g_launches{0};
 
 }  // namespace
+
+Tick2Geometry tick2_geometry() {
+    static const Tick2Geometry g = [] {
+        Tick2Geometry t{(uint32_t)kJit2RowsPerThread, (uint32_t)kJit2MaxThreads};
+        if (const char* v = std::getenv("CAVE_TICK2_ROWS")) {
+            const int r = std::atoi(v);
+            if (r >= 1 && r <= 3) t.rows_per_thread = (uint32_t)r;
+        }
+        if (const char* v = std::getenv("CAVE_TICK2_THREADS")) {
+            const int n = std::atoi(v);
+            if (n >= 32 && n <= 1024 && n % 32 == 0) t.max_threads = (uint32_t)n;
+        }
+        return t;
+    }();
+    return g;
+}
 
 JitMode jit_mode() {
     const char* v = std::getenv("CAVE_JIT");

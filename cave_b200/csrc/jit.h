@@ -83,6 +83,14 @@ cudaError_t launch_stream_tick2_jit(cudaKernel_t k, const StreamItem* items, uin
 // Dynamic shared memory of a two-tick launch with `rows` rows per CTA (incl. halo rows).
 size_t tick2_smem_bytes(uint32_t rows, uint32_t SX, uint32_t SXp);
 
+// Rows per thread and most threads per CTA of the two-tick kernels: kJit2RowsPerThread and
+// kJit2MaxThreads unless CAVE_TICK2_ROWS (1..3) / CAVE_TICK2_THREADS (a multiple of 32 up to 1024)
+// set them for the process (read once; the kernels are compiled with the same values).
+struct Tick2Geometry {
+    uint32_t rows_per_thread, max_threads;
+};
+Tick2Geometry tick2_geometry();
+
 // Process-wide counters behind cave_jit_stats.
 void jit_count_launch();
 void jit_counts(uint32_t* loaded, uint64_t* launches);

@@ -33,6 +33,9 @@ struct ResLaunch {           // geometry shared by every simulation of one launc
     uint32_t sxp_log2;       // lanes per row = 1 << sxp_log2 >= SX
     uint32_t nseg, seg_len;  // z-segments per CTA and planes per segment
     uint32_t n_sims;
+    uint32_t wait_us;        // limit of the wait for an initial grid's copy (0 = kWaitLimitNs)
+    uint32_t hold_init;      // failure test: the initial-grid copy is never issued, so the wait
+                             // runs out (only for launches of exactly one simulation)
 };
 struct ResSim {              // one simulation of a resident launch (24 bytes)
     const uint4* init;       // initial grid (strip layout, device memory, 16-byte aligned)

@@ -97,13 +97,14 @@ __global__ void __launch_bounds__(1024) k_resident(ResLaunch P, const ResSim* __
             uint4* rdst = reinterpret_cast<uint4*>(&s_rule);
             for (uint32_t i = tid; i < sizeof(DeviceRule) / 16; i += blockDim.x) rdst[i] = rsrc[i];
         }
-        if (tid == 0) {
+        if (tid == 0 && !P.hold_init) {
             fence_proxy_async();
             mbar_expect_tx(&s_bar, grid_bytes);
             bulk_g2s(grid, sd.init, grid_bytes, &s_bar);
         }
         uint32_t err = 0;
-        if (!mbar_wait_bounded(&s_bar, bar_phase, kWaitLimitNs)) err = kErrWaitTimeout;
+        if (!mbar_wait_bounded(&s_bar, bar_phase, P.wait_us ? (uint64_t)P.wait_us * 1000u : kWaitLimitNs))
+            err = kErrWaitTimeout;
         bar_phase ^= 1u;
         __syncthreads();  // rule visible
         DeviceRule R;

@@ -257,7 +257,7 @@ cudaError_t launch_stream_tick2_jit(cudaKernel_t k, const StreamItem* items, uin
                                     bool pdl, int tick_arg, int src_sel) {
     uint32_t lg = 0;
     while ((1u << lg) < SXp) lg++;
-    const size_t smem = stream2_smem_bytes(kJit2RowsPerThread * threads / SXp, SX, SXp);
+    const size_t smem = stream2_smem_bytes(tick2_geometry().rows_per_thread * threads / SXp, SX, SXp);
     {
         static std::mutex mu;
         static std::map<std::pair<const void*, int>, size_t> configured;

@@ -39,6 +39,7 @@ struct Request {
     std::vector<cave_sim_params> params;
     Clock::time_point submitted, finished;
     bool complete = false;
+    bool cancelled = false;  // cave_server_cancel: results are dropped as they arrive
 };
 
 }  // namespace
@@ -90,6 +91,13 @@ static void server_loop(cave_server* s) {
             auto it = s->requests.find(id);
             if (it == s->requests.end() || ix >= it->second.n) continue;
             Request& q = it->second;
+            if (q.cancelled) {  // a dropped simulation, or one that was running when cancelled
+                q.done++;
+                s->outstanding--;
+                if (!(r.result.error & kErrCancelled)) s->sims_completed++;
+                if (q.done == q.n) s->requests.erase(it);
+                continue;
+            }
             q.results[ix] = r.result;
             q.results[ix].params = q.params[ix];
             q.done++;
@@ -223,7 +231,7 @@ cave_status cave_server_wait(cave_server* s, uint64_t requestId, double timeoutS
     std::unique_lock<std::mutex> lock(s->mu);
     auto done = [&]() {
         auto it = s->requests.find(requestId);
-        return s->loop_rc != CAVE_OK || it == s->requests.end() || it->second.complete;
+        return s->loop_rc != CAVE_OK || it == s->requests.end() || it->second.complete || it->second.cancelled;
     };
     if (timeoutSeconds > 0) {
         if (!s->cv_done.wait_for(lock, std::chrono::duration<double>(timeoutSeconds), done)) return CAVE_ERR_TIMEOUT;
@@ -231,7 +239,29 @@ cave_status cave_server_wait(cave_server* s, uint64_t requestId, double timeoutS
         s->cv_done.wait(lock, done);
     }
     if (s->loop_rc) return s->loop_rc;
-    if (!s->requests.count(requestId)) return CAVE_ERR_INVALID_ARG;
+    auto it = s->requests.find(requestId);
+    if (it == s->requests.end() || it->second.cancelled) return CAVE_ERR_INVALID_ARG;
+    return CAVE_OK;
+}
+
+cave_status cave_server_cancel(cave_server* s, uint64_t requestId) {
+    if (!s) return CAVE_ERR_INVALID_ARG;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        auto it = s->requests.find(requestId);
+        if (it == s->requests.end() || it->second.cancelled) return CAVE_ERR_INVALID_ARG;
+        Request& q = it->second;
+        s->ready.erase(std::remove(s->ready.begin(), s->ready.end(), requestId), s->ready.end());
+        if (q.complete) {  // finished already: its results are discarded
+            s->requests.erase(it);
+            return CAVE_OK;
+        }
+        q.cancelled = true;
+        q.results.clear();
+    }
+    s->engine->cancel(requestId << kIndexBits, (requestId + 1) << kIndexBits);
+    s->cv_done.notify_all();
+    s->cv_work.notify_all();
     return CAVE_OK;
 }
 
@@ -240,7 +270,7 @@ cave_status cave_server_fetch(cave_server* s, uint64_t requestId, cave_sim_resul
     if (!s) return CAVE_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lock(s->mu);
     auto it = s->requests.find(requestId);
-    if (it == s->requests.end()) return CAVE_ERR_INVALID_ARG;
+    if (it == s->requests.end() || it->second.cancelled) return CAVE_ERR_INVALID_ARG;
     if (!it->second.complete) return CAVE_ERR_NOT_READY;
     if (n != it->second.n || !out) return CAVE_ERR_INVALID_ARG;
     std::memcpy(out, it->second.results.data(), sizeof(cave_sim_result) * n);

@@ -385,6 +385,12 @@ cave_status cave_server_poll(cave_server* s, uint64_t* requestIds, uint64_t cap,
 /* Blocks until the request has completed (timeoutSeconds <= 0: no limit; CAVE_ERR_TIMEOUT
  * when the time ran out). */
 cave_status cave_server_wait(cave_server* s, uint64_t requestId, double timeoutSeconds);
+/* Cancels a request (the reference's stop request, searchMode.cpp:437-449, for one request):
+ * its simulations not yet admitted leave the queue at once, those already on the device run to
+ * completion and their results are dropped; a completed request's results are discarded. After
+ * the call the id is unknown to wait / fetch (CAVE_ERR_INVALID_ARG), and requests submitted
+ * before or after it are unaffected. CAVE_ERR_INVALID_ARG for an unknown id. */
+cave_status cave_server_cancel(cave_server* s, uint64_t requestId);
 /* Copies a completed request's results (n = its simulation count, submission order, params in
  * the submitted form) and releases it; *latencySeconds = submit to completion. */
 cave_status cave_server_fetch(cave_server* s, uint64_t requestId, cave_sim_result* out, uint64_t n,

@@ -115,3 +115,30 @@ def test_batch_device_seeded_inits(ctx):
     for s in range(3):
         init = O.seed(G, G, G, spawn=(16, 16, 16), random=True, threshold=thr, run_seed=s, max_cell_state=3)
         assert got(res[s]) == expected(G, G, G, O.make_params(3, 3, 0x60, 0x70), init, 20)
+
+
+def test_withheld_initial_copy_times_out_without_a_fault(ctx, monkeypatch):
+    """Failure path of the bounded device waits: with the failure test switch the resident
+    kernel never issues a one-simulation batch's initial-grid copy, gives up its wait after 1 ms
+    and raises the timeout flag; the batch reports CAVE_ERR_TIMEOUT and the context stays usable
+    (a normal batch right after gives the oracle's result)."""
+    G = 21
+    init = O.seed(G, G, G, spawn=(9, 9, 9), random=True, threshold=O.threshold_from_float(0.35), run_seed=1,
+                  max_cell_state=3)
+    params = cb.make_params(3, 0x3, 0x60, 0x70)
+    monkeypatch.setenv("CAVE_TEST_WITHHOLD_INIT_COPY", "1")
+    with cb.Batch(ctx) as b:
+        ix = b.add_init(G, G, G, init)
+        b.add_sims([cb.SimDesc(params, ix, 10, 0, 0)])
+        b.launch()
+        with pytest.raises(cb.CaveError) as e:
+            b.results_array()
+        assert e.value.code == cb.ERR_TIMEOUT
+    monkeypatch.delenv("CAVE_TEST_WITHHOLD_INIT_COPY")
+    with cb.Batch(ctx) as b:
+        ix = b.add_init(G, G, G, init)
+        b.add_sims([cb.SimDesc(params, ix, 10, 0, 0)])
+        b.launch()
+        r = b.results_array()
+    want = O.run_sim(G, G, G, O.make_params(3, 0x3, 0x60, 0x70), init, 10, fast=True)[0]
+    assert tuple(int(v) for v in r[0]["info"]) == want.as_tuple()

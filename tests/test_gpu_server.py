@@ -141,3 +141,47 @@ def test_poll_reports_each_request_once(ctx):
         for rid in ids:
             s.fetch(rid)
     assert sorted(seen) == sorted(ids)
+
+
+def test_cancel_queued_and_running_requests(ctx):
+    """cave_server_cancel: a request queued behind others leaves the queue without running; a
+    request cancelled while on the device finishes unreported; the others complete with the
+    results they have alone, and the server's accounting stays consistent."""
+    rng = np.random.default_rng(41)
+    first = make_request(rng, 6, edges=(100,))
+    queued = make_request(rng, 5, edges=(70,))
+    later = make_request(rng, 4, edges=(40,))
+    alone_first = run_alone(ctx, first, hbm_budget=1 << 30)
+    alone_later = run_alone(ctx, later, hbm_budget=1 << 30)
+    with cb.Server(ctx, hbm_budget=1 << 30, max_active_cells=1, ticks_per_round=1) as s:  # one simulation at a time
+        a = s.submit(first)
+        q = s.submit(queued)
+        s.cancel(q)  # still behind `first`: dropped from the queue
+        with pytest.raises(cb.CaveError) as e:
+            s.wait(q, 1.0)
+        assert e.value.code == cb.ERR_INVALID_ARG
+        c = s.submit(later)
+        assert s.wait(a, 300.0) and s.wait(c, 300.0)
+        ra, _ = s.fetch(a)
+        rc_, _ = s.fetch(c)
+        st = s.stats()
+        assert st.completed == 2 and st.simsCompleted == first.size + later.size
+        # a request cancelled while it runs
+        b = s.submit(make_request(rng, 6, edges=(100,)))
+        time.sleep(0.02)
+        s.cancel(b)
+        d = s.submit(later)
+        assert s.wait(d, 300.0)
+        rd, _ = s.fetch(d)
+    for i in range(first.size):
+        assert as_tuple(ra[i]) == as_tuple(alone_first[i]), f"first sim {i}"
+    for i in range(later.size):
+        assert as_tuple(rc_[i]) == as_tuple(alone_later[i]), f"later sim {i}"
+        assert as_tuple(rd[i]) == as_tuple(alone_later[i]), f"later (again) sim {i}"
+
+
+def test_cancel_unknown_request_is_an_error(ctx):
+    with cb.Server(ctx, hbm_budget=1 << 28) as s:
+        with pytest.raises(cb.CaveError) as e:
+            s.cancel(12345)
+        assert e.value.code == cb.ERR_INVALID_ARG
