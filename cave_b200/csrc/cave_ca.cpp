@@ -612,23 +612,35 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
         if (!run_plan(ctx, g, rows_hint, kind, cps, env_cps != nullptr, plan))
             return set_error(ctx, CAVE_ERR_INTERNAL, "streaming plan failed");
     }
-    // tile shape: an override, the context's earlier choice for this shape, or a timing pass
+    // tile shape (and, with the rule-specialised kernels, one or two ticks per launch): an
+    // override, the context's earlier choice for this shape, or a timing pass
     if (e == cudaSuccess && !rows_hint && nticks >= kTuneMinTicks && (uint64_t)g->X * g->Y * g->Z >= kJitMinCells) {
         const TuneKey key{g->X, g->Y, g->Z, (d.flags & 7u) + 8u * kind};
-        uint32_t rows = 0;
+        RunChoice choice{};
         {
             std::lock_guard<std::mutex> lk(ctx->tune_mu);
             auto it = ctx->run_rows.find(key);
-            if (it != ctx->run_rows.end()) rows = it->second;
+            if (it != ctx->run_rows.end()) choice = it->second;
         }
-        if (!rows) {
-            std::vector<StreamPlan> cands;
+        if (!choice.rows) {
+            // candidates of the kernel kind in use and, when that is the two-tick kind, of the
+            // single-tick specialised kernels too; compared per tick
+            struct Cand {
+                uint32_t kind;
+                StreamPlan plan;
+            };
+            std::vector<Cand> cands;
             size_t most = 0;
-            for (uint32_t r : row_candidates(ctx, g->X, g->Y, plan.rows, kind)) {
-                StreamPlan c;
-                if (!run_plan(ctx, g, r, kind, cps, env_cps != nullptr, c)) continue;
-                most = std::max(most, c.items.size());
-                cands.push_back(std::move(c));
+            const uint32_t kinds[2] = {kind, kind == kRunJitPair ? (uint32_t)kRunJit : kind};
+            for (int ki = 0; ki < (kinds[1] != kinds[0] ? 2 : 1); ki++) {
+                StreamPlan base;
+                if (!run_plan(ctx, g, 0, kinds[ki], cps, env_cps != nullptr, base)) continue;
+                for (uint32_t r : row_candidates(ctx, g->X, g->Y, base.rows, kinds[ki])) {
+                    Cand c{kinds[ki], {}};
+                    if (!run_plan(ctx, g, r, kinds[ki], cps, env_cps != nullptr, c.plan)) continue;
+                    most = std::max(most, c.plan.items.size());
+                    cands.push_back(std::move(c));
+                }
             }
             cudaEvent_t e0 = nullptr, e1 = nullptr;
             StreamItem* titems = nullptr;
@@ -636,27 +648,32 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
             if (e == cudaSuccess) e = cudaEventCreate(&e1);
             if (e == cudaSuccess) e = cudaMalloc(&titems, sizeof(StreamItem) * std::max<size_t>(most, 1));
             float best = 1e30f;
-            for (const StreamPlan& c : cands) {
+            choice = RunChoice{kind, plan.rows};
+            for (const Cand& c : cands) {
                 float ms = 0;
-                if (e == cudaSuccess) e = time_plan(ctx, g, kind, s.rule, jk, c, titems, e0, e1, &ms);
-                if (e == cudaSuccess && c.rows == plan.rows) ms *= 0.98f;  // a challenger must beat the default by 2%
+                if (e == cudaSuccess) e = time_plan(ctx, g, c.kind, s.rule, jk, c.plan, titems, e0, e1, &ms);
+                if (c.kind == kRunJitPair) ms *= 0.5f;  // two ticks per launch
+                if (e == cudaSuccess && c.kind == kind && c.plan.rows == plan.rows)
+                    ms *= 0.98f;  // a challenger must beat the default by 2%
                 if (e == cudaSuccess && ms < best) {
                     best = ms;
-                    rows = c.rows;
+                    choice = RunChoice{c.kind, c.plan.rows};
                 }
             }
             if (e0) cudaEventDestroy(e0);
             if (e1) cudaEventDestroy(e1);
             cudaFree(titems);
-            if (e == cudaSuccess)
-                e = cudaMemsetAsync(dtt, 0, sizeof(TickTotals) * (kind == kRunJitPair ? 2 : 1), ctx->stream);
+            if (e == cudaSuccess) e = cudaMemsetAsync(dtt, 0, sizeof(TickTotals) * 2, ctx->stream);
             if (e == cudaSuccess) {
                 std::lock_guard<std::mutex> lk(ctx->tune_mu);
-                ctx->run_rows[key] = rows;
+                ctx->run_rows[key] = choice;
             }
         }
-        if (e == cudaSuccess && rows != plan.rows && !run_plan(ctx, g, rows, kind, cps, env_cps != nullptr, plan))
-            return set_error(ctx, CAVE_ERR_INTERNAL, "tile shape chosen by the timing pass could not be planned");
+        if (e == cudaSuccess && (choice.kind != kind || choice.rows != plan.rows)) {
+            kind = choice.kind;
+            if (!run_plan(ctx, g, choice.rows, kind, cps, env_cps != nullptr, plan))
+                return set_error(ctx, CAVE_ERR_INTERNAL, "tile shape chosen by the timing pass could not be planned");
+        }
     }
     // an odd tick count with the two-tick kernels: tick 0 alone first, with the single-tick plan
     StreamPlan plan1;

@@ -23,6 +23,10 @@ struct ExecChoice {
         return resident == o.resident && nseg == o.nseg && rows == o.rows && cells == o.cells;
     }
 };
+// cave_run's choice for a grid shape: tick kernel kind (cave_ca.cpp RunKind) and rows per CTA.
+struct RunChoice {
+    uint32_t kind = 0, rows = 0;
+};
 // Tuning-cache key: grid shape and neighbourhood bits.
 struct TuneKey {
     uint32_t X, Y, Z, nb;
@@ -56,9 +60,9 @@ struct cave_ctx {
     // autotuner results, shared by every batch and server of the context
     std::mutex tune_mu;
     std::map<cave::TuneKey, cave::ExecChoice> tune_cache;
-    // cave_run's tile choice (rows per CTA) per grid shape and tick kernel (key nb: neighbourhood
-    // bits, + 8 for the rule-specialised kernel), found by a short timing pass (cave_ca.cpp)
-    std::map<cave::TuneKey, uint32_t> run_rows;
+    // cave_run's tick kernel kind and tile (rows per CTA) per grid shape and the kernels available
+    // (key nb: neighbourhood bits + 8 x the default kind), found by a short timing pass (cave_ca.cpp)
+    std::map<cave::TuneKey, cave::RunChoice> run_rows;
     // engine staging buffers released by finished engines, reused by the next (freed with the context)
     std::mutex staging_mu;
     std::vector<cave::StagingPair> staging_free;

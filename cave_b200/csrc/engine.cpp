@@ -30,7 +30,25 @@ bool resident_fits(uint32_t X, uint32_t Y, uint32_t Z) {
     return resident_smem_bytes(X, Y, Z, 1) <= kMaxResidentSmem;
 }
 
-// Segments of ~8-12 planes (or nseg_hint), <= 1024 threads, within the shared-memory cap.
+// Registers a resident-kernel thread holds (its __launch_bounds__(1024) caps it at 64).
+constexpr uint32_t kResidentRegs = 64;
+
+static uint32_t resident_threads(uint32_t cols, uint32_t nseg) { return (nseg * cols + 31u) / 32u * 32u; }
+
+// CTAs of a resident geometry that fit one SM together: by shared memory (228 KB per SM, about
+// 3 KB of static shared memory and reserve per CTA), registers (64K per SM) and threads.
+static uint32_t resident_fit(uint32_t X, uint32_t Y, uint32_t Z, uint32_t nseg, uint32_t threads) {
+    const size_t smem = resident_smem_bytes(X, Y, Z, nseg);
+    const uint32_t by_smem = (uint32_t)((228u * 1024u) / (smem + 3 * 1024u));
+    const uint32_t by_regs = 65536u / (threads * kResidentRegs);
+    const uint32_t by_threads = 2048u / threads;
+    return std::max(1u, std::min({by_smem, by_regs, by_threads, 32u}));
+}
+
+// z-segments of a resident launch (or nseg_hint; CAVE_RESIDENT_NSEG overrides for tuning runs),
+// within 1024 threads and the shared-memory cap: preferring counts that fit two or more CTAs per
+// SM (each CTA waits at a barrier every plane; a second one fills those waits), then the most
+// threads resident per SM, then the most segments (the shortest march per tick).
 ResLaunch resident_geometry(uint32_t X, uint32_t Y, uint32_t Z, uint32_t nseg_hint, uint32_t& threads) {
     ResLaunch P{};
     P.X = X;
@@ -45,20 +63,34 @@ ResLaunch resident_geometry(uint32_t X, uint32_t Y, uint32_t Z, uint32_t nseg_hi
     P.sxp_log2 = lg;
     const uint32_t cols = Y * SXp;
     const uint32_t most = std::max(1u, std::min<uint32_t>(1024u / cols, Z));
-    uint32_t nseg = nseg_hint ? std::min(nseg_hint, most) : std::min(most, std::max(1u, (Z + 7u) / 8u));
+    if (!nseg_hint) {
+        if (const char* v = std::getenv("CAVE_RESIDENT_NSEG")) nseg_hint = (uint32_t)std::max(0, std::atoi(v));
+    }
+    uint32_t nseg = 1;
+    if (nseg_hint) {
+        nseg = std::min(nseg_hint, most);
+    } else {
+        uint64_t best = 0;
+        for (uint32_t k = 1; k <= most; k++) {
+            if (k > 1 && resident_smem_bytes(X, Y, Z, k) > kMaxResidentSmem) break;
+            const uint32_t t = resident_threads(cols, k);
+            const uint32_t fit = resident_fit(X, Y, Z, k, t);
+            const uint64_t score = ((uint64_t)std::min(fit, 2u) << 32) | ((uint64_t)(fit * t) << 8) | k;
+            if (score >= best) {
+                best = score;
+                nseg = k;
+            }
+        }
+    }
     while (nseg > 1 && resident_smem_bytes(X, Y, Z, nseg) > kMaxResidentSmem) nseg--;
     P.nseg = nseg;
     P.seg_len = (Z + nseg - 1) / nseg;
-    threads = (nseg * cols + 31u) / 32u * 32u;
+    threads = resident_threads(cols, nseg);
     return P;
 }
 
 uint32_t resident_ctas_per_sm(const ResLaunch& P, uint32_t threads) {
-    const size_t smem = resident_smem_bytes(P.X, P.Y, P.Z, P.nseg);
-    // 228 KB of shared memory per SM, about 3 KB of static shared memory and reserve per CTA
-    const uint32_t by_smem = std::max<uint32_t>(1u, (uint32_t)((228u * 1024u) / (smem + 3 * 1024u)));
-    const uint32_t by_threads = std::max<uint32_t>(1u, 2048u / threads);
-    return std::min(by_smem, by_threads);
+    return resident_fit(P.X, P.Y, P.Z, P.nseg, threads);
 }
 
 bool plan_tiled(uint32_t sim_index, uint32_t X, uint32_t Y, uint32_t Z, const ExecChoice& c, StreamPlan& plan) {
