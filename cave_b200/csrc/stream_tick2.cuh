@@ -171,6 +171,9 @@ __device__ __forceinline__ void stream_tick2_body(const StreamItem* __restrict__
         my_dst[q] = dst + ((size_t)max(y[q], 0) * SX + sx);
     }
     uint4* my_x = xch + (size_t)yy0 * SXp + sx;  // row q at + q * SXp; stage B at + kXch * xpar
+    // offsets of the rows above and below this thread's rows in an exchange buffer, clamped to
+    // its own row at the tile's first and last thread rows (whose results are not used)
+    const size_t x_dn = yy0 > 0 ? (size_t)SXp : 0, x_up = yy0 + kStrips < rows ? (size_t)kStrips * SXp : 0;
     const size_t plane_stride = (size_t)Y * SX;
     const size_t xpar = (size_t)rows * SXp;
 
@@ -238,7 +241,10 @@ __device__ __forceinline__ void stream_tick2_body(const StreamItem* __restrict__
             fence_proxy_async();
             issue(f + kRing);
         }
-        // ---- stage A: A(f - 1), plane zA
+        // ---- stage A: A(f - 1), plane zA. Every row is computed and rows stage A does not own
+        // are masked to 0 afterwards (a branch per row would split the step into blocks the
+        // compiler cannot interleave); the neighbour-row reads of edge rows are clamped in-bounds
+        // and their results discarded.
         uint4 nA1[kStrips];
         if (actA) {
             const int jA = f - 1;
@@ -247,56 +253,55 @@ __device__ __forceinline__ void stream_tick2_body(const StreamItem* __restrict__
             const bool ownA = !checked || (jA >= 2 && jA <= L + 1);
 #pragma unroll
             for (int q = 0; q < kStrips; q++) {
-                nA1[q] = make_uint4(0, 0, 0, 0);
-                if (rowA[q] && inA) {
-                    uint32_t psm[4], psp[4];
-                    if (q == 0) {
-                        const uint4 t = *(xa - SXp);
-                        psm[0] = t.x; psm[1] = t.y; psm[2] = t.z; psm[3] = t.w;
-                    } else {
+                uint32_t psm[4], psp[4];
+                if (q == 0) {
+                    const uint4 t = *(xa - x_dn);
+                    psm[0] = t.x; psm[1] = t.y; psm[2] = t.z; psm[3] = t.w;
+                } else {
 #pragma unroll
-                        for (int i = 0; i < P::NS; i++) psm[i] = psA[q - 1][i];
-                    }
-                    if (q == kStrips - 1) {
-                        const uint4 t = *(xa + (size_t)kStrips * SXp);
-                        psp[0] = t.x; psp[1] = t.y; psp[2] = t.z; psp[3] = t.w;
-                    } else {
-#pragma unroll
-                        for (int i = 0; i < P::NS; i++) psp[i] = psA[q + 1][i];
-                    }
-                    uint32_t cnt[count_bits(NB)];
-                    P::combine(pcA[q], psm, psp, cnt);
-                    nA1[q] = update_strip<NB, 0, kFirst, Fixed::kFullRange, kFirst ? kPopNone : kPopInput>(
-                        sAc[q], rAc[q].a, cnt, valid, R, accA, xbA[q], (uint32_t)zA, own[q] && ownA);
+                    for (int i = 0; i < P::NS; i++) psm[i] = psA[q - 1][i];
                 }
+                if (q == kStrips - 1) {
+                    const uint4 t = *(xa + x_up);
+                    psp[0] = t.x; psp[1] = t.y; psp[2] = t.z; psp[3] = t.w;
+                } else {
+#pragma unroll
+                    for (int i = 0; i < P::NS; i++) psp[i] = psA[q + 1][i];
+                }
+                uint32_t cnt[count_bits(NB)];
+                P::combine(pcA[q], psm, psp, cnt);
+                const uint4 n = update_strip<NB, 0, kFirst, Fixed::kFullRange, kFirst ? kPopNone : kPopInput>(
+                    sAc[q], rAc[q].a, cnt, valid, R, accA, xbA[q], (uint32_t)zA, own[q] && ownA);
+                const bool keep = rowA[q] && inA;
+                nA1[q] = keep ? n : make_uint4(0, 0, 0, 0);
             }
         }
-        // ---- stage B: B(f - 3), plane zB, written to HBM
+        // ---- stage B: B(f - 3), plane zB, written to HBM (rows it owns; the others computed and
+        // dropped, as in stage A)
         if (actB) {
             const int zB = zfirst + (f - 3) * zstep;
 #pragma unroll
             for (int q = 0; q < kStrips; q++) {
-                if (own[q]) {
-                    uint32_t psm[4], psp[4];
-                    if (q == 0) {
-                        const uint4 t = *(xb - SXp);
-                        psm[0] = t.x; psm[1] = t.y; psm[2] = t.z; psm[3] = t.w;
-                    } else {
+                uint32_t psm[4], psp[4];
+                if (q == 0) {
+                    const uint4 t = *(xb - x_dn);
+                    psm[0] = t.x; psm[1] = t.y; psm[2] = t.z; psm[3] = t.w;
+                } else {
 #pragma unroll
-                        for (int i = 0; i < P::NS; i++) psm[i] = psB[q - 1][i];
-                    }
-                    if (q == kStrips - 1) {
-                        const uint4 t = *(xb + (size_t)kStrips * SXp);
-                        psp[0] = t.x; psp[1] = t.y; psp[2] = t.z; psp[3] = t.w;
-                    } else {
-#pragma unroll
-                        for (int i = 0; i < P::NS; i++) psp[i] = psB[q + 1][i];
-                    }
-                    uint32_t cnt[count_bits(NB)];
-                    P::combine(pcB[q], psm, psp, cnt);
-                    my_dst[q][(size_t)zB * plane_stride] = update_strip<NB, 0, false, Fixed::kFullRange, kPopInput>(
-                        nA3[q], rBc[q].a, cnt, valid, R, accB, xbB[q], (uint32_t)zB);
+                    for (int i = 0; i < P::NS; i++) psm[i] = psB[q - 1][i];
                 }
+                if (q == kStrips - 1) {
+                    const uint4 t = *(xb + x_up);
+                    psp[0] = t.x; psp[1] = t.y; psp[2] = t.z; psp[3] = t.w;
+                } else {
+#pragma unroll
+                    for (int i = 0; i < P::NS; i++) psp[i] = psB[q + 1][i];
+                }
+                uint32_t cnt[count_bits(NB)];
+                P::combine(pcB[q], psm, psp, cnt);
+                const uint4 n = update_strip<NB, 0, false, Fixed::kFullRange, kPopInput>(
+                    nA3[q], rBc[q].a, cnt, valid, R, accB, xbB[q], (uint32_t)zB, own[q]);
+                if (own[q]) my_dst[q][(size_t)zB * plane_stride] = n;
             }
         }
         // ---- rotate
