@@ -803,6 +803,11 @@ def uneven_workload(args, world, rank, local, pg, steps, warmup):
         "plan": plan,
         "autotune_and_warmup_wall_s": tune_wall,
         "plain_path": plain,
+        # the whole batch against the plain path's rate on its every-64th sample (a 32-simulation
+        # batch cannot fill the GPU, so the same-sample ratio understates batching)
+        "batched_over_plain": ((n_all / (kern / 1e3)) / plain["plain_sims_per_s"]) if plain else None,
+        "batched_over_plain_cell_updates": ((upd_all / (kern / 1e3)) / plain["plain_cell_updates_per_s"])
+        if plain else None,
         "parity": parity,
         "e2e": {"value": n_all / (tot / 1e3), "unit": "sims/s", "h2d_bytes_per_step": int(len(mine) * 40),
                 "d2h_bytes_per_step": int(len(mine) * cb.SIM_RESULT_DTYPE.itemsize)},
