@@ -192,9 +192,6 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
         my_dst[q] = dst + ((size_t)max(y[q], 0) * SX + sx);
     }
     uint4* my_x = xch + (size_t)yy0 * SXp + sx;  // row q at + q * SXp
-    // offsets of the rows above and below this thread's rows in an exchange buffer, clamped to
-    // its own row at the tile's first and last thread rows (whose results are not used)
-    const size_t x_dn = yy0 > 0 ? (size_t)SXp : 0, x_up = yy0 + kStrips < rows ? (size_t)kStrips * SXp : 0;
     const size_t plane_stride = (size_t)Y * SX;
     const size_t xpar = (size_t)rows * SXp;
 
@@ -257,31 +254,30 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
             fence_proxy_async();
             issue(f + kRing);
         }
-        // every row is computed (a branch per row would split the step into blocks the compiler
-        // cannot interleave); rows the thread does not output are neither stored nor counted, and
-        // their clamped neighbour-row reads stay in bounds
 #pragma unroll
         for (int q = 0; q < kStrips; q++) {
-            uint32_t psm[4], psp[4];
-            if (q == 0) {
-                const uint4 t = *(xb - x_dn);
-                psm[0] = t.x; psm[1] = t.y; psm[2] = t.z; psm[3] = t.w;
-            } else {
+            if (outp[q]) {
+                uint32_t psm[4], psp[4];
+                if (q == 0) {
+                    const uint4 t = *(xb - SXp);
+                    psm[0] = t.x; psm[1] = t.y; psm[2] = t.z; psm[3] = t.w;
+                } else {
 #pragma unroll
-                for (int i = 0; i < P::NS; i++) psm[i] = ps[q - 1][i];
-            }
-            if (q == kStrips - 1) {
-                const uint4 t = *(xb + x_up);
-                psp[0] = t.x; psp[1] = t.y; psp[2] = t.z; psp[3] = t.w;
-            } else {
+                    for (int i = 0; i < P::NS; i++) psm[i] = ps[q - 1][i];
+                }
+                if (q == kStrips - 1) {
+                    const uint4 t = *(xb + (size_t)kStrips * SXp);
+                    psp[0] = t.x; psp[1] = t.y; psp[2] = t.z; psp[3] = t.w;
+                } else {
 #pragma unroll
-                for (int i = 0; i < P::NS; i++) psp[i] = ps[q + 1][i];
+                    for (int i = 0; i < P::NS; i++) psp[i] = ps[q + 1][i];
+                }
+                uint32_t cnt[count_bits(NB)];
+                P::combine(pc[q], psm, psp, cnt);
+                my_dst[q][(size_t)zo * plane_stride] =
+                    update_strip<NB, NT, kCountZero, Fixed::kFullRange, kPop>(s_c[q], r_c[q].a, cnt, valid, R, acc,
+                                                                                xbits[q], (uint32_t)zo);
             }
-            uint32_t cnt[count_bits(NB)];
-            P::combine(pc[q], psm, psp, cnt);
-            const uint4 n = update_strip<NB, NT, kCountZero, Fixed::kFullRange, kPop>(s_c[q], r_c[q].a, cnt, valid, R,
-                                                                                   acc, xbits[q], (uint32_t)zo, outp[q]);
-            if (outp[q]) my_dst[q][(size_t)zo * plane_stride] = n;
         }
 #pragma unroll
         for (int q = 0; q < kStrips; q++) {
