@@ -430,13 +430,16 @@ def large_workload(args, world, rank, local, pg, G, T, steps, warmup, e2e=True, 
         "ticks_per_launch": 2 if pairs else 1,
         "convert_ms_per_step": sum(conv_ms) / len(conv_ms),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "traffic": committed_traffic(f"stream_tick_{G}"),
+                     "peak_kind": peak_kind,
+                     # DRAM bytes per tick from the committed ncu summary of the kernel that ran
+                     "traffic": (lambda t: t / 2 if (t is not None and pairs) else t)(
+                         committed_traffic(f"stream_tick2_{G}" if pairs else f"stream_tick_{G}")),
                      "note": "algorithmic bytes = 1 B per cell update (packed 4-bit state read once, written once "
                              "per tick); achieved = G^3 B x ticks / tick-loop time (CUDA events on the library's "
-                             "stream)" + ("; two ticks per launch: the grid crosses HBM once per two ticks, so the "
-                                          "achieved rate can exceed the copy bandwidth and `traffic` (DRAM bytes "
-                                          "per launch, ncu) is about half the algorithmic bytes of its two ticks"
-                                          if pairs else "")},
+                             "stream); traffic = ncu DRAM bytes (read + write) per tick of the same kernel"
+                             + ("; two ticks per launch: the grid crosses HBM once per two ticks, so traffic is "
+                                "about half the algorithmic bytes and the achieved rate may exceed the copy "
+                                "bandwidth" if pairs else "")},
         "parity": ({"ok": True, "checked": f"last timed run{' and last end-to-end run' if e2e else ''}: every cell, "
                                           f"every tick's statistics and the GridInfo equal "
                                           f"tests/golden/large_fixtures.json ({G}^3, {T} ticks)"}
