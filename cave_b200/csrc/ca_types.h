@@ -35,7 +35,11 @@ constexpr int kJitMaxThreads = kJitRowsPerThread == 2 ? 512 : 384;
 #ifndef CAVE_TICK2_THREADS
 #define CAVE_TICK2_THREADS 384
 #endif
+#ifndef CAVE_TICK2_CTAS
+#define CAVE_TICK2_CTAS 1
+#endif
 constexpr int kJit2RowsPerThread = CAVE_TICK2_ROWS;
+constexpr int kJit2CtasPerSm = CAVE_TICK2_CTAS;  // CTAs per SM the kernels' registers are sized for
 constexpr int kJit2MaxThreads = CAVE_TICK2_THREADS;
 
 constexpr int kMaxTerms = 8;        // capacity of DeviceRule::terms

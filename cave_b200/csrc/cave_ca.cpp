@@ -448,8 +448,10 @@ static uint32_t kind_max_threads(uint32_t kind) {
     return kind == kRunGeneric ? 1024u : kind == kRunJit ? (uint32_t)kJitMaxThreads : tick2_geometry().max_threads;
 }
 // Dynamic shared memory the two-tick kernels may take (their static share is a few KB).
-static bool pair_smem_fits(const cave_ctx* ctx, const StreamPlan& p) {
-    return tick2_smem_bytes(p.rows, p.SX, p.SXp) + 4096 <= (size_t)ctx->smem_optin;
+static bool pair_smem_fits(const cave_ctx* ctx, const StreamPlan& p, uint32_t per_sm = 1) {
+    const size_t need = tick2_smem_bytes(p.rows, p.SX, p.SXp) + 4096;
+    // one CTA: the opt-in limit; several: their share of the SM's 228 KB
+    return per_sm <= 1 ? need <= (size_t)ctx->smem_optin : need * per_sm <= 228u * 1024u;
 }
 
 // The plan of one cave_run tile shape: `rows` per CTA (0 = default) for tick kernels of `kind`.
@@ -461,18 +463,19 @@ static bool run_plan(const cave_ctx* ctx, const cave_grid* g, uint32_t rows, uin
     const uint32_t sms = (uint32_t)ctx->sm_count;
     const uint32_t spt = kind_spt(kind), halo = kind_halo(kind), most = kind_max_threads(kind);
     if (kind == kRunGeneric) return plan_stream(0, g->X, g->Y, g->Z, sms * cps, rows, plan, 1);
-    if (!plan_stream(0, g->X, g->Y, g->Z, sms * (cps_given ? cps : 1u), rows, plan, spt, halo, most)) return false;
+    // CTAs per SM the kernels are built for (the two-tick kernels may be built for several)
+    const uint32_t per_sm = cps_given ? cps : kind == kRunJitPair ? tick2_geometry().ctas_per_sm : 1u;
+    if (!plan_stream(0, g->X, g->Y, g->Z, sms * per_sm, rows, plan, spt, halo, most)) return false;
     if (kind == kRunJitPair) {
         const uint32_t step = std::max(1u, 32u / plan.SXp) * spt;
-        while (!pair_smem_fits(ctx, plan)) {
+        while (!pair_smem_fits(ctx, plan, per_sm)) {
             if (plan.rows < 2 * halo + 1 + step) return false;
-            if (!plan_stream(0, g->X, g->Y, g->Z, sms * (cps_given ? cps : 1u), plan.rows - step, plan, spt, halo,
-                             most))
-                return false;
+            if (!plan_stream(0, g->X, g->Y, g->Z, sms * per_sm, plan.rows - step, plan, spt, halo, most)) return false;
         }
     }
     if (!cps_given && plan.threads < most)
-        return plan_stream(0, g->X, g->Y, g->Z, sms * (most / plan.threads), plan.rows, plan, spt, halo, most);
+        return plan_stream(0, g->X, g->Y, g->Z, sms * per_sm * (most / plan.threads), plan.rows, plan, spt, halo,
+                           most);
     return true;
 }
 
@@ -492,7 +495,7 @@ static std::vector<uint32_t> row_candidates(const cave_ctx* ctx, uint32_t X, uin
             p.rows = r;
             p.SX = SX;
             p.SXp = SXp;
-            if (!pair_smem_fits(ctx, p)) continue;
+            if (!pair_smem_fits(ctx, p, tick2_geometry().ctas_per_sm)) continue;
         }
         const uint64_t tiles = (Y + (r - 2 * halo) - 1) / (r - 2 * halo);
         scored.push_back({tiles * r, r});
@@ -689,6 +692,13 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
         e = cudaMemcpyAsync(ditems + n_main, plan1.items.data(), sizeof(StreamItem) * n_lead, cudaMemcpyHostToDevice,
                             ctx->stream);
     // The tick launches. A launch reads cell copy `sel` and writes the other one.
+    // CAVE_RUN_GRAPH=1 (a measurement mode) captures them into a CUDA graph and replays it; the
+    // tick timing then covers the replay alone (instantiation falls in convert_ms).
+    const char* env_graph = std::getenv("CAVE_RUN_GRAPH");
+    const bool use_graph = env_graph && !std::strcmp(env_graph, "1") && nticks > 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    if (use_graph && e == cudaSuccess) e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed);
     uint32_t sel = 0, launches = 0;
     if (kind == kRunJitPair) {
         uint32_t t = 0;
@@ -709,6 +719,13 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
         sel = nticks & 1u;
         launches = nticks;
     }
+    if (use_graph) {
+        const cudaError_t ec = cudaStreamEndCapture(ctx->stream, &graph);
+        if (e == cudaSuccess) e = ec;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&gexec, graph, 0);
+        record(ctx, 2);
+        if (e == cudaSuccess) e = cudaGraphLaunch(gexec, ctx->stream);
+    }
     if (e == cudaSuccess && nticks && jk)  // the last tick's population comes from the final grid
         e = launch_strip_stats(g->strips + (uint64_t)sel * nstrips, g->Y, g->Z, plan.SX, dtt + (nticks - 1),
                                (uint32_t)ctx->sm_count, ctx->stream);
@@ -726,6 +743,8 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
         e = cudaMemcpyAsync(per_tick, dticks, sizeof(cave_tick_stats) * nticks, cudaMemcpyDeviceToHost, ctx->stream);
     record(ctx, 5);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
     cudaFree(dticks);
     cudaFree(ditems);
     cudaFree(dtt);

@@ -70,7 +70,7 @@ CAVE_JIT_KERNEL(cave_stream_tick_jit_derived, false, false)
 CAVE_JIT_KERNEL(cave_stream_tick_jit_dense, true, true)
 CAVE_JIT_KERNEL(cave_stream_tick_jit_dense_derived, false, true)
 #define CAVE_JIT_KERNEL2(NAME, FIRST, DENSE)                                                              \
-    extern "C" __global__ void __launch_bounds__(cave::kJit2MaxThreads, 1)                                 \
+    extern "C" __global__ void __launch_bounds__(cave::kJit2MaxThreads, cave::kJit2CtasPerSm)              \
         NAME(const cave::StreamItem* __restrict__ items, cave::StripSim* sims, uint4* pool, uint32_t sxp_log2, \
              int tick_arg, int src_sel) {                                                                  \
         cave::stream_tick2_body<CAVE_JIT_NB, cave::JitRule, FIRST, DENSE, cave::kJit2RowsPerThread>(       \
@@ -180,7 +180,8 @@ std::vector<std::string> options_for(const JitKey& k) {
     // -default-device: the C header's declarations (host functions) are parsed as device ones
     return {"--gpu-architecture=sm_100a", "-std=c++20", "-default-device", "-lineinfo", b[0], b[1], b[2], b[3],
             "-DCAVE_TICK2_ROWS=" + std::to_string(tick2_geometry().rows_per_thread),
-            "-DCAVE_TICK2_THREADS=" + std::to_string(tick2_geometry().max_threads)};
+            "-DCAVE_TICK2_THREADS=" + std::to_string(tick2_geometry().max_threads),
+            "-DCAVE_TICK2_CTAS=" + std::to_string(tick2_geometry().ctas_per_sm)};
 }
 
 // Compiles the kernel for k (or reads it from the disk cache). No device is touched.
@@ -378,7 +379,11 @@ std::atomic<uint64_t> g_launches{0};
 
 Tick2Geometry tick2_geometry() {
     static const Tick2Geometry g = [] {
-        Tick2Geometry t{(uint32_t)kJit2RowsPerThread, (uint32_t)kJit2MaxThreads};
+        Tick2Geometry t{(uint32_t)kJit2RowsPerThread, (uint32_t)kJit2MaxThreads, (uint32_t)kJit2CtasPerSm};
+        if (const char* v = std::getenv("CAVE_TICK2_CTAS")) {
+            const int c = std::atoi(v);
+            if (c >= 1 && c <= 4) t.ctas_per_sm = (uint32_t)c;
+        }
         if (const char* v = std::getenv("CAVE_TICK2_ROWS")) {
             const int r = std::atoi(v);
             if (r >= 1 && r <= 3) t.rows_per_thread = (uint32_t)r;

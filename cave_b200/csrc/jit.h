@@ -83,11 +83,12 @@ cudaError_t launch_stream_tick2_jit(cudaKernel_t k, const StreamItem* items, uin
 // Dynamic shared memory of a two-tick launch with `rows` rows per CTA (incl. halo rows).
 size_t tick2_smem_bytes(uint32_t rows, uint32_t SX, uint32_t SXp);
 
-// Rows per thread and most threads per CTA of the two-tick kernels: kJit2RowsPerThread and
-// kJit2MaxThreads unless CAVE_TICK2_ROWS (1..3) / CAVE_TICK2_THREADS (a multiple of 32 up to 1024)
-// set them for the process (read once; the kernels are compiled with the same values).
+// Rows per thread, most threads per CTA and CTAs per SM of the two-tick kernels:
+// kJit2RowsPerThread, kJit2MaxThreads and kJit2CtasPerSm unless CAVE_TICK2_ROWS (1..3),
+// CAVE_TICK2_THREADS (a multiple of 32 up to 1024) or CAVE_TICK2_CTAS (1..4) set them for the
+// process (read once; the kernels are compiled with the same values).
 struct Tick2Geometry {
-    uint32_t rows_per_thread, max_threads;
+    uint32_t rows_per_thread, max_threads, ctas_per_sm;
 };
 Tick2Geometry tick2_geometry();
 

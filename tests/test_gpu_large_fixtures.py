@@ -75,3 +75,17 @@ def test_large_grid_run_host_buffers(ctx, monkeypatch, name):
         g.upload(np.zeros_like(init))  # the run must take its input from the host buffer
         ticks, info = g.run_host(pin_in.data_ptr(), pin_out.data_ptr(), params, T, T)
         _check(name, T, pin_out.numpy().view(np.uint32), ticks, info)
+
+
+@pytest.mark.parametrize("pairs", ["1", "0"])
+def test_tick_loop_replayed_from_a_graph(ctx, monkeypatch, pairs):
+    """CAVE_RUN_GRAPH=1 (a measurement mode): the tick launches captured into a CUDA graph and
+    replayed give the same cells, statistics and GridInfo."""
+    monkeypatch.setenv("CAVE_JIT", "sync")
+    monkeypatch.setenv("CAVE_RUN_GRAPH", "1")
+    monkeypatch.setenv("CAVE_TICK2", pairs)
+    name, T = "active256", 100
+    g, params = _setup(ctx, name)
+    with g:
+        ticks, info = g.run(params, T, T)
+        _check(name, T, g.download(), ticks, info)
