@@ -139,14 +139,14 @@ class BatchOptions(ctypes.Structure):
 
 class ServerOptions(ctypes.Structure):
     _fields_ = [("hbmBudget", u64), ("maxInFlight", u32), ("ticksPerRound", u32), ("autotune", u32),
-                ("tiledOnly", u32), ("maxActiveCells", u64)]
+                ("tiledOnly", u32), ("maxActiveCells", u64), ("requestDeadlineSeconds", ctypes.c_double)]
 
 
 class ServerStats(ctypes.Structure):
     _fields_ = [("submitted", u64), ("completed", u64), ("simsCompleted", u64), ("cellUpdates", u64),
                 ("p50LatencySeconds", ctypes.c_double), ("p99LatencySeconds", ctypes.c_double),
                 ("busySeconds", ctypes.c_double), ("peakBytes", u64), ("rounds", u64), ("tickLaunches", u64),
-                ("residentLaunches", u64), ("tuneMs", ctypes.c_double)]
+                ("residentLaunches", u64), ("tuneMs", ctypes.c_double), ("expired", u64)]
 
 
 REQUEST_SIM_DTYPE = np.dtype([("X", "<u4"), ("Y", "<u4"), ("Z", "<u4"), ("maxTicks", "<u4"), ("birth", "<u8"),
@@ -596,10 +596,10 @@ class Server:
     """Sweep requests served as they arrive (cave_server): continuous batching on one GPU."""
 
     def __init__(self, ctx: Context, hbm_budget=0, max_in_flight=0, ticks_per_round=0, autotune=False,
-                 tiled_only=False, max_active_cells=0):
+                 tiled_only=False, max_active_cells=0, request_deadline=0.0):
         self.ctx = ctx
         o = ServerOptions(hbm_budget, max_in_flight, ticks_per_round, 1 if autotune else 0, 1 if tiled_only else 0,
-                          max_active_cells)
+                          max_active_cells, request_deadline)
         h = ctypes.c_void_p()
         ctx.check(lib().cave_server_create(ctx.h, ctypes.byref(o), ctypes.byref(h)), "cave_server_create")
         self.h = h

@@ -13,11 +13,13 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <new>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -40,6 +42,7 @@ struct Request {
     Clock::time_point submitted, finished;
     bool complete = false;
     bool cancelled = false;  // cave_server_cancel: results are dropped as they arrive
+    bool expired = false;    // past the deadline: results are dropped, wait / fetch time out
 };
 
 }  // namespace
@@ -52,19 +55,27 @@ struct cave_server {
     std::condition_variable cv_work, cv_done;
     bool stop = false;
     cave_status loop_rc = CAVE_OK;
+    std::string loop_msg;             // why the scheduler thread stopped
+    double deadline_s = 0;            // requestDeadlineSeconds (0 = none)
+    uint64_t fail_after_rounds = 0;   // CAVE_TEST_SERVER_FAIL_AFTER_ROUNDS (0 = never)
+    uint64_t rounds = 0;
     uint64_t next_id = 1;
     std::map<uint64_t, Request> requests;
-    std::vector<uint64_t> ready;      // completed, not yet reported by poll
+    std::vector<uint64_t> ready;      // completed or expired, not yet reported by poll
     std::vector<double> latencies;    // seconds, per completed request
-    uint64_t submitted = 0, completed = 0, sims_completed = 0, cell_updates = 0;
+    uint64_t submitted = 0, completed = 0, sims_completed = 0, cell_updates = 0, expired = 0;
     uint64_t outstanding = 0;         // simulations submitted and not finished
     double busy_s = 0;
     Clock::time_point busy_since;
 };
 
+// The scheduler thread's error, as the caller's status and last error text.
+static cave_status loop_error(cave_server* s) { return set_error(s->ctx, s->loop_rc, s->loop_msg); }
+
 static void server_loop(cave_server* s) {
     cudaSetDevice(s->ctx->device);
     std::vector<EngineResult> res;
+    std::vector<uint64_t> expire;
     for (;;) {
         {
             std::unique_lock<std::mutex> lock(s->mu);
@@ -75,13 +86,25 @@ static void server_loop(cave_server* s) {
                 if (s->outstanding == 0) continue;
             }
         }
+        if (s->fail_after_rounds && s->rounds >= s->fail_after_rounds) {
+            // host-side failure injection (tests): the scheduler stops between rounds with the
+            // device work of earlier rounds still queued; destroy waits for it
+            std::lock_guard<std::mutex> lock(s->mu);
+            s->loop_rc = CAVE_ERR_INTERNAL;
+            s->loop_msg = "scheduler thread stopped: failure injected after " + std::to_string(s->rounds) + " rounds";
+            s->cv_done.notify_all();
+            break;
+        }
         bool idle = false;
         const cave_status rc = s->engine->step(&idle);
+        s->rounds++;
         res.clear();
         s->engine->take_results(res);
-        std::lock_guard<std::mutex> lock(s->mu);
+        expire.clear();
+        std::unique_lock<std::mutex> lock(s->mu);
         if (rc) {
             s->loop_rc = rc;
+            s->loop_msg = std::string("scheduler thread stopped: ") + cave_last_error(s->ctx);
             s->cv_done.notify_all();
             break;
         }
@@ -91,11 +114,11 @@ static void server_loop(cave_server* s) {
             auto it = s->requests.find(id);
             if (it == s->requests.end() || ix >= it->second.n) continue;
             Request& q = it->second;
-            if (q.cancelled) {  // a dropped simulation, or one that was running when cancelled
+            if (q.cancelled || q.expired) {  // dropped, or running when cancelled / expired
                 q.done++;
                 s->outstanding--;
                 if (!(r.result.error & kErrCancelled)) s->sims_completed++;
-                if (q.done == q.n) s->requests.erase(it);
+                if (q.done == q.n && q.cancelled) s->requests.erase(it);
                 continue;
             }
             q.results[ix] = r.result;
@@ -111,8 +134,22 @@ static void server_loop(cave_server* s) {
                 s->ready.push_back(id);
             }
         }
+        if (s->deadline_s > 0) {  // watchdog: requests past their deadline expire
+            for (auto& [id, q] : s->requests) {
+                if (q.complete || q.cancelled || q.expired ||
+                    std::chrono::duration<double>(now - q.submitted).count() <= s->deadline_s)
+                    continue;
+                q.expired = true;
+                q.results.clear();
+                s->expired++;
+                s->ready.push_back(id);
+                expire.push_back(id);
+            }
+        }
         if (s->outstanding == 0) s->busy_s += std::chrono::duration<double>(now - s->busy_since).count();
-        if (!res.empty()) s->cv_done.notify_all();
+        if (!res.empty() || !expire.empty()) s->cv_done.notify_all();
+        lock.unlock();
+        for (const uint64_t id : expire) s->engine->cancel(id << kIndexBits, (id + 1) << kIndexBits);
     }
 }
 
@@ -133,6 +170,8 @@ cave_status cave_server_create(cave_ctx* ctx, const cave_server_options* opt, ca
     cave_server* s = new (std::nothrow) cave_server();
     if (!s) return CAVE_ERR_OUT_OF_MEMORY;
     s->ctx = ctx;
+    s->deadline_s = o.requestDeadlineSeconds > 0 ? o.requestDeadlineSeconds : 0;
+    if (const char* e = std::getenv("CAVE_TEST_SERVER_FAIL_AFTER_ROUNDS")) s->fail_after_rounds = std::strtoull(e, nullptr, 10);
     EngineConfig ec;
     ec.pool_bytes = budget;
     ec.max_slots = o.maxInFlight ? o.maxInFlight : (1u << 14);
@@ -173,7 +212,7 @@ cave_status cave_server_submit(cave_server* s, const cave_request_sim* sims, uin
     uint64_t id;
     {
         std::lock_guard<std::mutex> lock(s->mu);
-        if (s->loop_rc) return s->loop_rc;
+        if (s->loop_rc) return loop_error(s);
         id = s->next_id++;
     }
     for (uint64_t i = 0; i < n; i++) {
@@ -223,7 +262,7 @@ cave_status cave_server_poll(cave_server* s, uint64_t* requestIds, uint64_t cap,
     std::copy(s->ready.begin(), s->ready.begin() + k, requestIds);
     s->ready.erase(s->ready.begin(), s->ready.begin() + k);
     *n = k;
-    return s->loop_rc;
+    return s->loop_rc ? loop_error(s) : CAVE_OK;
 }
 
 cave_status cave_server_wait(cave_server* s, uint64_t requestId, double timeoutSeconds) {
@@ -231,17 +270,19 @@ cave_status cave_server_wait(cave_server* s, uint64_t requestId, double timeoutS
     std::unique_lock<std::mutex> lock(s->mu);
     auto done = [&]() {
         auto it = s->requests.find(requestId);
-        return s->loop_rc != CAVE_OK || it == s->requests.end() || it->second.complete || it->second.cancelled;
+        return s->loop_rc != CAVE_OK || it == s->requests.end() || it->second.complete || it->second.cancelled ||
+               it->second.expired;
     };
     if (timeoutSeconds > 0) {
         if (!s->cv_done.wait_for(lock, std::chrono::duration<double>(timeoutSeconds), done)) return CAVE_ERR_TIMEOUT;
     } else {
         s->cv_done.wait(lock, done);
     }
-    if (s->loop_rc) return s->loop_rc;
     auto it = s->requests.find(requestId);
-    if (it == s->requests.end() || it->second.cancelled) return CAVE_ERR_INVALID_ARG;
-    return CAVE_OK;
+    if (it == s->requests.end() || it->second.cancelled) return s->loop_rc ? loop_error(s) : CAVE_ERR_INVALID_ARG;
+    if (it->second.complete) return CAVE_OK;  // results that arrived before a scheduler failure stand
+    if (it->second.expired) return set_error(s->ctx, CAVE_ERR_TIMEOUT, "request passed its deadline");
+    return loop_error(s);
 }
 
 cave_status cave_server_cancel(cave_server* s, uint64_t requestId) {
@@ -252,12 +293,14 @@ cave_status cave_server_cancel(cave_server* s, uint64_t requestId) {
         if (it == s->requests.end() || it->second.cancelled) return CAVE_ERR_INVALID_ARG;
         Request& q = it->second;
         s->ready.erase(std::remove(s->ready.begin(), s->ready.end(), requestId), s->ready.end());
-        if (q.complete) {  // finished already: its results are discarded
+        if (q.complete || (q.expired && q.done == q.n)) {  // nothing still to arrive
             s->requests.erase(it);
             return CAVE_OK;
         }
+        const bool was_expired = q.expired;  // its queue was cancelled when it expired
         q.cancelled = true;
         q.results.clear();
+        if (was_expired) return CAVE_OK;
     }
     s->engine->cancel(requestId << kIndexBits, (requestId + 1) << kIndexBits);
     s->cv_done.notify_all();
@@ -271,7 +314,13 @@ cave_status cave_server_fetch(cave_server* s, uint64_t requestId, cave_sim_resul
     std::lock_guard<std::mutex> lock(s->mu);
     auto it = s->requests.find(requestId);
     if (it == s->requests.end() || it->second.cancelled) return CAVE_ERR_INVALID_ARG;
-    if (!it->second.complete) return CAVE_ERR_NOT_READY;
+    if (it->second.expired) {  // released: results still in flight are dropped as they arrive
+        s->ready.erase(std::remove(s->ready.begin(), s->ready.end(), requestId), s->ready.end());
+        if (it->second.done == it->second.n) s->requests.erase(it);
+        else it->second.cancelled = true;
+        return set_error(s->ctx, CAVE_ERR_TIMEOUT, "request passed its deadline");
+    }
+    if (!it->second.complete) return s->loop_rc ? loop_error(s) : CAVE_ERR_NOT_READY;
     if (n != it->second.n || !out) return CAVE_ERR_INVALID_ARG;
     std::memcpy(out, it->second.results.data(), sizeof(cave_sim_result) * n);
     if (latencySeconds)
@@ -308,8 +357,9 @@ cave_status cave_server_get_stats(cave_server* s, cave_server_stats* out) {
     st.tickLaunches = es.tick_launches;
     st.residentLaunches = es.resident_launches;
     st.tuneMs = es.tune_ms;
+    st.expired = s->expired;
     *out = st;
-    return s->loop_rc;
+    return s->loop_rc ? loop_error(s) : CAVE_OK;
 }
 
 }  // extern "C"

@@ -360,6 +360,10 @@ typedef struct {
                                    cells (0 = 2^31, several ticks of work for the GPU): the
                                    oldest requests run first instead of every request
                                    sharing the GPU; ~0 = limited by memory only            */
+    double requestDeadlineSeconds; /* a request not complete this long after its submission
+                                   expires (0 = never): its queued simulations leave the
+                                   queue, running ones finish unreported, and wait / fetch
+                                   return CAVE_ERR_TIMEOUT (fetch releases it)              */
 } cave_server_options;
 
 typedef struct {
@@ -372,6 +376,7 @@ typedef struct {
     uint64_t peakBytes;                 /* largest grid memory in use                       */
     uint64_t rounds, tickLaunches, residentLaunches;
     double tuneMs;                      /* host time spent autotuning                       */
+    uint64_t expired;                   /* requests that passed requestDeadlineSeconds      */
 } cave_server_stats;
 
 cave_status cave_server_create(cave_ctx* ctx, const cave_server_options* options, cave_server** out);
@@ -380,10 +385,12 @@ void cave_server_destroy(cave_server* s);
 /* Queues a request of n simulations (non-blocking) and returns its id. Fails with
  * CAVE_ERR_OUT_OF_MEMORY when one simulation alone needs more than the budget. */
 cave_status cave_server_submit(cave_server* s, const cave_request_sim* sims, uint64_t n, uint64_t* requestId);
-/* Ids of requests that completed since the last poll (up to cap). Non-blocking. */
+/* Ids of requests that completed or expired since the last poll (up to cap). Non-blocking. */
 cave_status cave_server_poll(cave_server* s, uint64_t* requestIds, uint64_t cap, uint64_t* n);
 /* Blocks until the request has completed (timeoutSeconds <= 0: no limit; CAVE_ERR_TIMEOUT
- * when the time ran out). */
+ * when the time ran out, or when the request passed requestDeadlineSeconds). When the
+ * scheduler thread has failed, submit, poll and stats return its error, and so do wait and
+ * fetch for a request that had not completed (completed results can still be fetched). */
 cave_status cave_server_wait(cave_server* s, uint64_t requestId, double timeoutSeconds);
 /* Cancels a request (the reference's stop request, searchMode.cpp:437-449, for one request):
  * its simulations not yet admitted leave the queue at once, those already on the device run to
@@ -392,7 +399,8 @@ cave_status cave_server_wait(cave_server* s, uint64_t requestId, double timeoutS
  * before or after it are unaffected. CAVE_ERR_INVALID_ARG for an unknown id. */
 cave_status cave_server_cancel(cave_server* s, uint64_t requestId);
 /* Copies a completed request's results (n = its simulation count, submission order, params in
- * the submitted form) and releases it; *latencySeconds = submit to completion. */
+ * the submitted form) and releases it; *latencySeconds = submit to completion. An expired
+ * request returns CAVE_ERR_TIMEOUT and is released (the id becomes unknown). */
 cave_status cave_server_fetch(cave_server* s, uint64_t requestId, cave_sim_result* out, uint64_t n,
                               double* latencySeconds);
 cave_status cave_server_get_stats(cave_server* s, cave_server_stats* out);

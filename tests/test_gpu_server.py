@@ -185,3 +185,81 @@ def test_cancel_unknown_request_is_an_error(ctx):
         with pytest.raises(cb.CaveError) as e:
             s.cancel(12345)
         assert e.value.code == cb.ERR_INVALID_ARG
+
+
+def long_request(n, edge=256, ticks=300):
+    """n copies of a simulation that stays alive for all its ticks (Moore S{3,4} B{4}, C = 16)."""
+    r = cb.request_sims(n)
+    p = O.make_params(16, 0x7, 1 << 4, (1 << 3) | (1 << 4))
+    for i in range(n):
+        r[i]["X"] = r[i]["Y"] = r[i]["Z"] = edge
+        r[i]["maxTicks"] = ticks
+        r[i]["birth"], r[i]["survival"] = int(p[0]), int(p[1])
+        r[i]["spawnX"] = r[i]["spawnY"] = r[i]["spawnZ"] = edge
+        r[i]["runSeedIndex"] = 11
+        r[i]["threshold"] = O.threshold_from_float(0.35)
+        r[i]["tag"] = i
+    return r
+
+
+def test_request_deadline_expires_and_later_requests_run(ctx):
+    """requestDeadlineSeconds: a request still running past its deadline expires -- wait stops
+    waiting, poll reports it, fetch returns CAVE_ERR_TIMEOUT and releases it, its queued
+    simulations never run -- while a request submitted afterwards completes with the results it
+    has alone."""
+    rng = np.random.default_rng(43)
+    small = make_request(rng, 4, edges=(24, 33))
+    alone = run_alone(ctx, small, hbm_budget=1 << 30)
+    big = long_request(200)  # one at a time: seconds of work
+    with cb.Server(ctx, hbm_budget=1 << 30, max_active_cells=1, ticks_per_round=1, request_deadline=1.0) as s:
+        t0 = time.time()
+        rid = s.submit(big)
+        assert not s.wait(rid, 60.0)
+        waited = time.time() - t0
+        assert 1.0 <= waited < 10.0, waited
+        assert rid in s.poll()
+        with pytest.raises(cb.CaveError) as e:
+            s.fetch(rid)
+        assert e.value.code == cb.ERR_TIMEOUT and "deadline" in str(e.value)
+        with pytest.raises(cb.CaveError) as e:  # released: the id is unknown now
+            s.cancel(rid)
+        assert e.value.code == cb.ERR_INVALID_ARG
+        q = s.submit(small)
+        assert s.wait(q, 60.0)
+        res, _ = s.fetch(q)
+        st = s.stats()
+        assert st.expired == 1 and st.completed == 1
+        assert st.simsCompleted < big.size + small.size  # the expired request's queue was dropped
+    for i in range(small.size):
+        assert as_tuple(res[i]) == as_tuple(alone[i]), f"sim {i}"
+
+
+def test_cancel_of_an_expired_request_releases_it(ctx):
+    with cb.Server(ctx, hbm_budget=1 << 30, max_active_cells=1, ticks_per_round=1, request_deadline=0.2) as s:
+        rid = s.submit(long_request(50))
+        assert not s.wait(rid, 60.0)
+        s.cancel(rid)
+        with pytest.raises(cb.CaveError) as e:
+            s.wait(rid, 1.0)
+        assert e.value.code == cb.ERR_INVALID_ARG
+        assert s.stats().expired == 1
+
+
+def test_injected_scheduler_failure_reaches_every_waiter(ctx, monkeypatch):
+    """A scheduler thread that stops (failure injected on the host between rounds, with device
+    work still queued) is reported to wait, poll, submit and fetch instead of leaving them
+    blocked; the server shuts down cleanly and the context serves a new server."""
+    monkeypatch.setenv("CAVE_TEST_SERVER_FAIL_AFTER_ROUNDS", "3")
+    rng = np.random.default_rng(47)
+    with cb.Server(ctx, hbm_budget=1 << 30, max_active_cells=1, ticks_per_round=1) as s:
+        rid = s.submit(long_request(6, edge=100, ticks=50))  # needs hundreds of rounds
+        for call in (lambda: s.wait(rid, 60.0), lambda: s.poll(), lambda: s.submit(make_request(rng, 2)),
+                     lambda: s.fetch(rid)):
+            with pytest.raises(cb.CaveError) as e:
+                call()
+            assert e.value.code == cb.ERR_INTERNAL and "failure injected after 3 rounds" in str(e.value)
+    monkeypatch.delenv("CAVE_TEST_SERVER_FAIL_AFTER_ROUNDS")
+    req = make_request(rng, 3, edges=(24, 40))
+    res = run_alone(ctx, req, hbm_budget=1 << 30)
+    for i in range(req.size):
+        assert as_tuple(res[i]) == oracle_result(req[i]), f"sim {i}"
