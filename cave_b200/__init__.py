@@ -13,7 +13,8 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libcave_ca.so")
+# CAVE_LIB selects another build of the library, e.g. cave_b200/libcave_ca_checked.so
+LIB_PATH = os.environ.get("CAVE_LIB") or os.path.join(_HERE, "libcave_ca.so")
 HEADER_PATH = os.path.join(_HERE, "..", "include", "cave_ca.h")
 
 PERM_MASK = (1 << 60) - 1

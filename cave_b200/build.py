@@ -1,6 +1,11 @@
 """Builds cave_b200/libcave_ca.so in-tree (nvcc for .cu at sm_100a, g++ -std=c++20 for .cpp).
 
-Usage: python -m cave_b200.build [--force] [--verbose]
+With --checked it builds the checked library instead, cave_b200/libcave_ca_checked.so: every source
+(and the kernels it compiles at run time) with -DCAVE_CHECKED, so that the hot kernels test their
+shared- and global-memory indices and report a failed test as an error flag. Load it in place of the
+normal library with CAVE_LIB=<path>.
+
+Usage: python -m cave_b200.build [--force] [--verbose] [--checked]
 """
 from __future__ import annotations
 
@@ -14,6 +19,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libcave_ca.so")
+OBJ_CHECKED = os.path.join(HERE, "_build_checked")
+LIB_CHECKED = os.path.join(HERE, "libcave_ca_checked.so")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -37,9 +44,9 @@ JIT_SOURCES = [(n, os.path.join(CSRC, n)) for n in (
 _DELIM = "cave_jit_src"
 
 
-def _gen_jit_sources(force=False):
-    """Writes _build/jit_sources.cpp: the JIT headers as string literals (kJitSource*)."""
-    out = os.path.join(OBJ, "jit_sources.cpp")
+def _gen_jit_sources(obj_dir, force=False):
+    """Writes <obj_dir>/jit_sources.cpp: the JIT headers as string literals (kJitSource*)."""
+    out = os.path.join(obj_dir, "jit_sources.cpp")
     paths = [p for _, p in JIT_SOURCES] + [os.path.abspath(__file__)]
     if not force and not _stale(out, paths):
         return out
@@ -68,12 +75,12 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def _compile(src, verbose):
-    obj = os.path.join(OBJ, os.path.basename(src) + ".o")
+def _compile(src, obj_dir, defines, verbose):
+    obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
     if src.endswith(".cu"):
-        cmd = [NVCC] + NVCC_FLAGS + ["-c", src, "-o", obj]
+        cmd = [NVCC] + NVCC_FLAGS + defines + ["-c", src, "-o", obj]
     else:
-        cmd = [CXX] + CXX_FLAGS + ["-c", src, "-o", obj]
+        cmd = [CXX] + CXX_FLAGS + defines + ["-c", src, "-o", obj]
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -82,27 +89,29 @@ def _compile(src, verbose):
     return obj, r.stderr
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    os.makedirs(OBJ, exist_ok=True)
+def build(force: bool = False, verbose: bool = False, checked: bool = False) -> str:
+    obj_dir, lib = (OBJ_CHECKED, LIB_CHECKED) if checked else (OBJ, LIB)
+    defines = ["-DCAVE_CHECKED"] if checked else []
+    os.makedirs(obj_dir, exist_ok=True)
     srcs = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp")))
-    srcs.append(_gen_jit_sources(force))
+    srcs.append(_gen_jit_sources(obj_dir, force))
     hdrs = _headers()
-    todo = [s for s in srcs if force or _stale(os.path.join(OBJ, os.path.basename(s) + ".o"), [s] + hdrs)]
+    todo = [s for s in srcs if force or _stale(os.path.join(obj_dir, os.path.basename(s) + ".o"), [s] + hdrs)]
     if todo:
         with cf.ThreadPoolExecutor(max_workers=min(8, len(todo))) as ex:
-            for obj, err in ex.map(lambda s: _compile(s, verbose), todo):
+            for obj, err in ex.map(lambda s: _compile(s, obj_dir, defines, verbose), todo):
                 if err.strip() and verbose:
                     print(err, file=sys.stderr)
-    objs = [os.path.join(OBJ, os.path.basename(s) + ".o") for s in srcs]
-    if force or todo or _stale(LIB, objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart_static", "-lpthread", "-ldl", "-lrt"]
+    objs = [os.path.join(obj_dir, os.path.basename(s) + ".o") for s in srcs]
+    if force or todo or _stale(lib, objs):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", lib] + objs + ["-lcudart_static", "-lpthread", "-ldl", "-lrt"]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed\n{r.stdout}\n{r.stderr}")
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose="--verbose" in sys.argv))
+    print(build(force="--force" in sys.argv, verbose="--verbose" in sys.argv, checked="--checked" in sys.argv))

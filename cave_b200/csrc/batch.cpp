@@ -497,12 +497,13 @@ cave_status cave_batch_results(cave_batch* b, cave_sim_result* out, uint64_t n) 
                                                                       0xFFFFFFFFu);
         }
     }
-    bool err = false;
+    uint32_t err = 0;
     for (uint64_t i = 0; i < n; i++) {
         out[i].tag = b->sims[i].d.tag;
         out[i].params = b->translated[i];
-        err |= out[i].error != 0;
+        err |= out[i].error;
     }
+    if (err & kErrBounds) return set_error(ctx, CAVE_ERR_INTERNAL, "a batched simulation failed an index check");
     if (err) return set_error(ctx, CAVE_ERR_TIMEOUT, "a batched simulation raised a device error flag");
     return CAVE_OK;
 }

@@ -282,11 +282,14 @@ struct TickAcc {  // per-thread accumulators for one tick
 // kPop: where the population and bounding box come from -- kPopOutput: the strip's new state
 // (the tick's own); kPopInput: its current state, i.e. the previous tick's result, whose
 // non-zero mask the update computes anyway; kPopNone: not counted.
+// kZPerStrip: the z-extent (acc.zmin / zmax) is updated here for this strip; otherwise the
+// counted non-zero mask is ORed into *zany and the caller updates the extent once per plane.
 enum : int { kPopNone = 0, kPopOutput = 1, kPopInput = 2 };
-template <int NB, int NT, bool kCountZero = true, bool kFullRange = false, int kPop = kPopOutput>
+template <int NB, int NT, bool kCountZero = true, bool kFullRange = false, int kPop = kPopOutput,
+          bool kZPerStrip = true>
 __device__ __forceinline__ uint4 update_strip(uint4 s, uint32_t a, const uint32_t* cnt, uint32_t valid,
                                               const DeviceRule& r, TickAcc& acc, uint32_t& xbits, uint32_t z,
-                                              bool count = true) {
+                                              bool count = true, uint32_t* zany = nullptr) {
     uint32_t hs, hb;
     eval_rule<count_bits(NB), NT>(cnt, r, hs, hb);
     const uint32_t nz = s.x | s.y | s.z | s.w;
@@ -327,9 +330,13 @@ __device__ __forceinline__ uint4 update_strip(uint4 s, uint32_t a, const uint32_
             const uint32_t nn = kPop == kPopInput ? nz : (n.x | n.y | n.z | n.w);
             acc.population = mad_add(acc.population, __popc(nn), acc.one);
             xbits |= nn;
-            const bool any = nn != 0u;
-            acc.zmin = any ? min(acc.zmin, z) : acc.zmin;
-            acc.zmax = any ? max(acc.zmax, z) : acc.zmax;
+            if constexpr (kZPerStrip) {
+                const bool any = nn != 0u;
+                acc.zmin = any ? min(acc.zmin, z) : acc.zmin;
+                acc.zmax = any ? max(acc.zmax, z) : acc.zmax;
+            } else {
+                *zany |= nn;
+            }
         }
     }
     return n;

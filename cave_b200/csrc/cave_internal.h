@@ -16,7 +16,19 @@ constexpr uint64_t kPermMask = (uint64_t(1) << 60) - 1;  // simulation.h:43
 constexpr uint64_t kWaitLimitNs = 1000000000ull;
 
 // Error flags a kernel may raise in its record (read back by the host).
-enum : uint32_t { kErrNone = 0, kErrWaitTimeout = 1, kErrBadRuleIndex = 2, kErrCancelled = 4 };
+enum : uint32_t { kErrNone = 0, kErrWaitTimeout = 1, kErrBadRuleIndex = 2, kErrCancelled = 4, kErrBounds = 8 };
+
+// Index checks of the checked build (compiled with -DCAVE_CHECKED, libcave_ca_checked.so): the
+// hot kernels test every shared- and global-memory index against the extent it must stay in.
+// CAVE_IN_BOUNDS(i, n, err) is true when i < n; otherwise it raises kErrBounds in err (which
+// reaches the simulation record like any other error flag) and is false, and the caller skips
+// the access: a failed check neither faults nor traps. In the normal build it is the constant
+// true and its arguments are never evaluated.
+#ifdef CAVE_CHECKED
+#define CAVE_IN_BOUNDS(i, n, err) (((uint64_t)(i) < (uint64_t)(n)) ? true : (((err) |= cave::kErrBounds), false))
+#else
+#define CAVE_IN_BOUNDS(i, n, err) true
+#endif
 
 // Per-grid device record of the plain path. It holds what the reference keeps in the
 // per-slot permutation / snapshot / GridInfo / copy buffers (searchSystem.cpp:202-374).

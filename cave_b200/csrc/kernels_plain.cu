@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include "cave_internal.h"
+#include "ptx.cuh"
 
 namespace cave {
 
@@ -133,14 +134,11 @@ __global__ void __launch_bounds__(256) k_plain_step(PlainArgs A) {
     const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     uint32_t v[11] = {died, dying, born, surv, pop, bmin[0], bmin[1], bmin[2], bmax[0], bmax[1], bmax[2]};
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
+    for (int k = 0; k < 5; k++) v[k] = warp_add(v[k]);
 #pragma unroll
-        for (int k = 0; k < 5; k++) v[k] += __shfl_xor_sync(0xFFFFFFFFu, v[k], o);
+    for (int k = 5; k < 8; k++) v[k] = warp_min(v[k]);
 #pragma unroll
-        for (int k = 5; k < 8; k++) v[k] = min(v[k], __shfl_xor_sync(0xFFFFFFFFu, v[k], o));
-#pragma unroll
-        for (int k = 8; k < 11; k++) v[k] = max(v[k], __shfl_xor_sync(0xFFFFFFFFu, v[k], o));
-    }
+    for (int k = 8; k < 11; k++) v[k] = warp_max(v[k]);
     if (lane == 0) {
 #pragma unroll
         for (int k = 0; k < 11; k++) red[warp][k] = v[k];

@@ -81,6 +81,14 @@ __global__ void __launch_bounds__(1024) k_resident(ResLaunch P, const ResSim* __
     __syncthreads();
     uint32_t bar_phase = 0;
     const uint32_t grid_bytes = plane * Z * 16u;
+    // extents (uint4 units) that the checked build tests every index against; a layout that does
+    // not fit the launch's shared memory fails every shared-memory check
+    uint32_t layout_err = 0;
+    size_t grid_n = (size_t)plane * Z, xch_n = (size_t)2 * xpar;
+#ifdef CAVE_CHECKED
+    if (!CAVE_IN_BOUNDS((grid_n + xch_n) * 16 - 1, dynamic_smem_bytes(), layout_err)) grid_n = xch_n = 0;
+#endif
+    const size_t g_off = (size_t)yy * SX + sx, x_off = (size_t)seg * xseg + (size_t)(yy + 1) * SXp + sx;
 
     uint4* my_x = xch + (size_t)seg * xseg + (size_t)(yy + 1) * SXp + sx;
     uint4* my_g = grid + (size_t)yy * SX + sx;  // + z * plane
@@ -97,12 +105,16 @@ __global__ void __launch_bounds__(1024) k_resident(ResLaunch P, const ResSim* __
             uint4* rdst = reinterpret_cast<uint4*>(&s_rule);
             for (uint32_t i = tid; i < sizeof(DeviceRule) / 16; i += blockDim.x) rdst[i] = rsrc[i];
         }
+        uint32_t err = layout_err;
         if (tid == 0 && !P.hold_init) {
             fence_proxy_async();
-            mbar_expect_tx(&s_bar, grid_bytes);
-            bulk_g2s(grid, sd.init, grid_bytes, &s_bar);
+            if (CAVE_IN_BOUNDS(grid_bytes / 16u - 1u, grid_n, err)) {
+                mbar_expect_tx(&s_bar, grid_bytes);
+                bulk_g2s(grid, sd.init, grid_bytes, &s_bar);
+            } else {
+                mbar_arrive(&s_bar);  // checked build: the copy is skipped, its phase completed
+            }
         }
-        uint32_t err = 0;
         if (!mbar_wait_bounded(&s_bar, bar_phase, P.wait_us ? (uint64_t)P.wait_us * 1000u : kWaitLimitNs))
             err = kErrWaitTimeout;
         bar_phase ^= 1u;
@@ -117,7 +129,9 @@ __global__ void __launch_bounds__(1024) k_resident(ResLaunch P, const ResSim* __
         for (int t = 0; t < NT; t++) R.terms[t] = s_rule.terms[t];
 
         auto load = [&](int z) -> uint4 {
-            return (has && z >= 0 && z < (int)Z) ? my_g[(size_t)z * plane] : make_uint4(0, 0, 0, 0);
+            return (has && z >= 0 && z < (int)Z && CAVE_IN_BOUNDS(g_off + (size_t)z * plane, grid_n, err))
+                       ? my_g[(size_t)z * plane]
+                       : make_uint4(0, 0, 0, 0);
         };
         auto row_of = [&](uint4 st) -> Row {
             const uint32_t a = alive_plane(st, R);  // zero for absent strips
@@ -149,14 +163,17 @@ __global__ void __launch_bounds__(1024) k_resident(ResLaunch P, const ResSim* __
                 uint32_t pc[PS::NC], ps[PS::NS];
                 PS::make(r_m, r_c, r_p, pc, ps);
                 uint4* xb = my_x + (size_t)U * xpar;
-                if (in_seg) *xb = to_u4<PS::NS>(ps);
+                const size_t xi = x_off + (size_t)U * xpar;
+                if (in_seg && CAVE_IN_BOUNDS(xi, xch_n, err)) *xb = to_u4<PS::NS>(ps);
                 __syncthreads();
                 if (act && has) {
-                    const uint4 qm = *(xb - SXp), qp = *(xb + SXp);
+                    const uint4 qm = CAVE_IN_BOUNDS(xi - SXp, xch_n, err) ? *(xb - SXp) : make_uint4(0, 0, 0, 0);
+                    const uint4 qp = CAVE_IN_BOUNDS(xi + SXp, xch_n, err) ? *(xb + SXp) : make_uint4(0, 0, 0, 0);
                     const uint32_t psm[4] = {qm.x, qm.y, qm.z, qm.w}, psp[4] = {qp.x, qp.y, qp.z, qp.w};
                     uint32_t cnt[count_bits(NB)];
                     combine<NB>(pc, psm, psp, cnt);
-                    my_g[(size_t)z * plane] = update_strip<NB, NT>(s_c, r_c.a, cnt, valid, R, acc, xbits, (uint32_t)z);
+                    const uint4 n = update_strip<NB, NT>(s_c, r_c.a, cnt, valid, R, acc, xbits, (uint32_t)z);
+                    if (CAVE_IN_BOUNDS(g_off + (size_t)z * plane, grid_n, err)) my_g[(size_t)z * plane] = n;
                 }
                 r_m = r_c;
                 r_c = r_p;
@@ -178,16 +195,8 @@ __global__ void __launch_bounds__(1024) k_resident(ResLaunch P, const ResSim* __
             }
             uint32_t v[11] = {acc.surviving, acc.born, acc.zero, acc.population, bx0, by0, acc.zmin, bx1, by1,
                               acc.zmax, err};
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-                for (int q = 0; q < 4; q++) v[q] += __shfl_xor_sync(0xFFFFFFFFu, v[q], o);
-#pragma unroll
-                for (int q = 4; q < 7; q++) v[q] = min(v[q], __shfl_xor_sync(0xFFFFFFFFu, v[q], o));
-#pragma unroll
-                for (int q = 7; q < 10; q++) v[q] = max(v[q], __shfl_xor_sync(0xFFFFFFFFu, v[q], o));
-                v[10] |= __shfl_xor_sync(0xFFFFFFFFu, v[10], o);
-            }
+            warp_reduce_tick(v);
+            v[10] = warp_or(v[10]);
             const uint32_t lane = tid & 31u, warp = tid >> 5;
             if (lane == 0) {
 #pragma unroll
@@ -195,21 +204,13 @@ __global__ void __launch_bounds__(1024) k_resident(ResLaunch P, const ResSim* __
             }
             __syncthreads();
             if (warp == 0) {
-                // lane w takes warp w's values; then a shuffle reduction over the lanes
+                // lane w takes warp w's values; then a reduction over the lanes
                 const uint32_t nw = (blockDim.x + 31) >> 5;
                 const bool live = lane < nw;
 #pragma unroll
                 for (int q = 0; q < 11; q++) v[q] = live ? red[lane][q] : ((q >= 4 && q < 7) ? 0xFFFFFFFFu : 0u);
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-                    for (int q = 0; q < 4; q++) v[q] += __shfl_xor_sync(0xFFFFFFFFu, v[q], o);
-#pragma unroll
-                    for (int q = 4; q < 7; q++) v[q] = min(v[q], __shfl_xor_sync(0xFFFFFFFFu, v[q], o));
-#pragma unroll
-                    for (int q = 7; q < 10; q++) v[q] = max(v[q], __shfl_xor_sync(0xFFFFFFFFu, v[q], o));
-                    v[10] |= __shfl_xor_sync(0xFFFFFFFFu, v[10], o);
-                }
+                warp_reduce_tick(v);
+                v[10] = warp_or(v[10]);
             }
             if (tid == 0) {
                 const uint32_t surv = v[0], born = v[1], zero = v[2], pop = v[3];

@@ -120,14 +120,11 @@ __global__ void __launch_bounds__(256) k_strip_stats(const uint4* __restrict__ s
         v[3] = min(v[3], z);
         v[6] = max(v[6], z);
     }
+    v[0] = warp_add(v[0]);
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        v[0] += __shfl_xor_sync(0xFFFFFFFFu, v[0], o);
+    for (int q = 1; q < 4; q++) v[q] = warp_min(v[q]);
 #pragma unroll
-        for (int q = 1; q < 4; q++) v[q] = min(v[q], __shfl_xor_sync(0xFFFFFFFFu, v[q], o));
-#pragma unroll
-        for (int q = 4; q < 7; q++) v[q] = max(v[q], __shfl_xor_sync(0xFFFFFFFFu, v[q], o));
-    }
+    for (int q = 4; q < 7; q++) v[q] = warp_max(v[q]);
     const uint32_t warp = threadIdx.x >> 5;
     if ((threadIdx.x & 31u) == 0) {
         for (int q = 0; q < 7; q++) red[warp][q] = v[q];
@@ -283,6 +280,43 @@ cudaError_t launch_stream_tick2_jit(cudaKernel_t k, const StreamItem* items, uin
     cfg.attrs = attr;
     cfg.numAttrs = (pdl && stream_pdl()) ? 1 : 0;
     void* args[] = {(void*)&items, (void*)&sims, (void*)&pool, (void*)&lg, (void*)&tick_arg, (void*)&src_sel};
+    const cudaError_t e = cudaLaunchKernelExC(&cfg, (const void*)k, args);
+    if (e == cudaSuccess) jit_count_launch();
+    return e;
+}
+
+cudaError_t launch_stream_tick2_chain_jit(cudaKernel_t k, const StreamItem* items, uint32_t n_items, StripSim* sims,
+                                          uint4* pool, uint32_t SX, uint32_t SXp, uint32_t threads, cudaStream_t st,
+                                          int tick_arg, int src_sel, uint32_t npasses, uint32_t* flags, uint32_t ny) {
+    uint32_t lg = 0;
+    while ((1u << lg) < SXp) lg++;
+    const size_t smem = stream2_smem_bytes(tick2_geometry().rows_per_thread * threads / SXp, SX, SXp);
+    {
+        static std::mutex mu;
+        static std::map<std::pair<const void*, int>, size_t> configured;
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        std::lock_guard<std::mutex> lock(mu);
+        size_t& c = configured[{(const void*)k, dev}];
+        if (smem > c) {
+            e = cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            c = smem;
+        }
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(n_items);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;  // every CTA resident: they wait on one another
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    void* args[] = {(void*)&items, (void*)&sims, (void*)&pool, (void*)&lg, (void*)&tick_arg, (void*)&src_sel,
+                    (void*)&npasses, (void*)&flags, (void*)&ny};
     const cudaError_t e = cudaLaunchKernelExC(&cfg, (const void*)k, args);
     if (e == cudaSuccess) jit_count_launch();
     return e;

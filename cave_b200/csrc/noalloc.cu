@@ -159,6 +159,7 @@ extern "C" cave_status cave_run_noalloc(cave_ctx* ctx, const uint32_t* d_in, uin
     if (e == cudaSuccess) e = cudaMemcpyAsync(&back, rec_dev, sizeof(back), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) return check_cuda(ctx, e, "cave_run_noalloc");
+    if (back.error & kErrBounds) return set_error(ctx, CAVE_ERR_INTERNAL, "streaming kernel: an index check failed");
     if (back.error & kErrWaitTimeout)
         return set_error(ctx, CAVE_ERR_TIMEOUT, "streaming kernel: bulk-copy wait timed out");
     if (back.error) return set_error(ctx, CAVE_ERR_INTERNAL, "streaming kernel raised an error flag");

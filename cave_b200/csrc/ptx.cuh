@@ -30,6 +30,44 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
+// Dynamic shared memory of the launch, in bytes.
+__device__ __forceinline__ uint32_t dynamic_smem_bytes() {
+    uint32_t r;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(r));
+    return r;
+}
+// Warp-wide reductions (redux.sync, one instruction each) over all 32 lanes; every lane gets
+// the result. volatile: they must stay where all 32 lanes execute them.
+__device__ __forceinline__ uint32_t warp_add(uint32_t v) {
+    uint32_t r;
+    asm volatile("redux.sync.add.u32 %0, %1, 0xffffffff;" : "=r"(r) : "r"(v));
+    return r;
+}
+__device__ __forceinline__ uint32_t warp_min(uint32_t v) {
+    uint32_t r;
+    asm volatile("redux.sync.min.u32 %0, %1, 0xffffffff;" : "=r"(r) : "r"(v));
+    return r;
+}
+__device__ __forceinline__ uint32_t warp_max(uint32_t v) {
+    uint32_t r;
+    asm volatile("redux.sync.max.u32 %0, %1, 0xffffffff;" : "=r"(r) : "r"(v));
+    return r;
+}
+__device__ __forceinline__ uint32_t warp_or(uint32_t v) {
+    uint32_t r;
+    asm volatile("redux.sync.or.b32 %0, %1, 0xffffffff;" : "=r"(r) : "r"(v));
+    return r;
+}
+// One tick's per-thread statistics v[0..10) reduced over the warp: 0..3 sums, 4..6 minima,
+// 7..9 maxima (the bounding box).
+__device__ __forceinline__ void warp_reduce_tick(uint32_t* v) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) v[q] = warp_add(v[q]);
+#pragma unroll
+    for (int q = 4; q < 7; q++) v[q] = warp_min(v[q]);
+#pragma unroll
+    for (int q = 7; q < 10; q++) v[q] = warp_max(v[q]);
+}
 // Nanoseconds of the GPU's global timer.
 __device__ __forceinline__ uint64_t global_ns() {
     uint64_t t;
@@ -57,5 +95,19 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 }
 // Orders this thread's generic-proxy shared-memory accesses before later async-proxy ones.
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// The same for every state space: global data that generic stores wrote (and this thread has
+// acquired) before bulk copies read it.
+__device__ __forceinline__ void fence_proxy_async_all() { asm volatile("fence.proxy.async;" ::: "memory"); }
+__device__ __forceinline__ void mbar_inval(uint64_t* bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(uint32_t* p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
 }  // namespace cave

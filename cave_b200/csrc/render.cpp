@@ -116,6 +116,7 @@ cave_status cave_render_step(cave_ctx* ctx, const uint32_t* d_in, uint32_t* d_ou
     if (e == cudaSuccess) e = cudaMemcpyAsync(&back, rec, sizeof(back), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) return check_cuda(ctx, e, "cave_render_step");
+    if (back.error & kErrBounds) return set_error(ctx, CAVE_ERR_INTERNAL, "streaming kernel: an index check failed");
     if (back.error & kErrWaitTimeout) return set_error(ctx, CAVE_ERR_TIMEOUT, "streaming kernel: bulk-copy wait timed out");
     if (back.error) return set_error(ctx, CAVE_ERR_INTERNAL, "streaming kernel raised an error flag");
     if (back.tick != nticks) return set_error(ctx, CAVE_ERR_INTERNAL, "render step ran a different number of ticks");

@@ -327,8 +327,9 @@ cave_status cave_server_fetch(cave_server* s, uint64_t requestId, cave_sim_resul
         *latencySeconds = std::chrono::duration<double>(it->second.finished - it->second.submitted).count();
     s->ready.erase(std::remove(s->ready.begin(), s->ready.end(), requestId), s->ready.end());
     s->requests.erase(it);
-    bool err = false;
-    for (uint64_t i = 0; i < n; i++) err |= out[i].error != 0;
+    uint32_t err = 0;
+    for (uint64_t i = 0; i < n; i++) err |= out[i].error;
+    if (err & kErrBounds) return set_error(s->ctx, CAVE_ERR_INTERNAL, "a served simulation failed an index check");
     if (err) return set_error(s->ctx, CAVE_ERR_TIMEOUT, "a served simulation raised a device error flag");
     return CAVE_OK;
 }

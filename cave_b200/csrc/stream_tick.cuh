@@ -140,6 +140,16 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
     const bool down = (it.dir_items & 1u) != 0;
     const int zstep = down ? -1 : 1;
     const int zfirst = down ? (int)it.z1 : (int)it.z0 - 1;  // plane of fetch 0
+    uint32_t err = 0;
+    // extents (uint4 units) that the checked build tests every index against; a layout that does
+    // not fit the launch's shared memory fails every shared-memory check
+    const size_t xpar = (size_t)rows * SXp;
+    size_t ring_n = (size_t)kRing * slot_stride, xch_n = (size_t)kXch * xpar;
+    const size_t copy_n = (size_t)Z * Y * SX;
+#ifdef CAVE_CHECKED
+    if (!CAVE_IN_BOUNDS((ring_n + xch_n) * 16 + kRing * 8 - 1, dynamic_smem_bytes(), err)) ring_n = xch_n = 0;
+#endif
+    const size_t ring_off = (size_t)yy0 * SX + sx, x_off = (size_t)yy0 * SXp + sx;
 
     // Thread 0 fills ring slot f % kRing with input plane f. A plane outside the grid is not
     // copied; its slot's phase is completed by a plain arrive instead, so that every fetch
@@ -152,10 +162,14 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
             mbar_arrive(&bars[s]);
             return;
         }
-        uint4* slot = ring + (size_t)s * slot_stride + (size_t)slot_row0 * SX;
-        const uint4* g = src + ((size_t)p * Y + (size_t)ylo) * SX;
+        const size_t slot_i = (size_t)s * slot_stride + (size_t)slot_row0 * SX, g_i = ((size_t)p * Y + (size_t)ylo) * SX;
+        if (!CAVE_IN_BOUNDS(slot_i + tile_bytes / 16u - 1u, ring_n, err) ||
+            !CAVE_IN_BOUNDS(g_i + tile_bytes / 16u - 1u, copy_n, err)) {
+            mbar_arrive(&bars[s]);  // checked build: the copy is skipped, its phase completed
+            return;
+        }
         mbar_expect_tx(&bars[s], tile_bytes);
-        bulk_g2s(slot, g, tile_bytes, &bars[s]);
+        bulk_g2s(ring + slot_i, src + g_i, tile_bytes, &bars[s]);
     };
     const uint32_t producer = 0;  // the thread that issues the plane copies
     if (threadIdx.x == producer) {
@@ -170,11 +184,15 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
             if (!has[q]) {
 #pragma unroll
                 for (int s = 0; s < kRing; s++)
-                    const_cast<uint4*>(my_ring)[(size_t)s * slot_stride + (size_t)q * SX] = make_uint4(0, 0, 0, 0);
+                    if (CAVE_IN_BOUNDS(ring_off + (size_t)s * slot_stride + (size_t)q * SX, ring_n, err))
+                        const_cast<uint4*>(my_ring)[(size_t)s * slot_stride + (size_t)q * SX] = make_uint4(0, 0, 0, 0);
             }
         }
     }
-    uint32_t err = 0;
+    auto ring_ok = [&](int s, int q) {
+        return CAVE_IN_BOUNDS(ring_off + (size_t)s * slot_stride + (size_t)q * SX, ring_n, err);
+    };
+    auto x_ok = [&](size_t rel) { return CAVE_IN_BOUNDS(x_off + rel, xch_n, err); };
     auto row_of = [&](uint4 st) -> Row {
         const uint32_t a = alive_plane(st, R);  // zero for absent strips: state 0 is never alive
         const uint32_t v = a & send_mask;
@@ -193,7 +211,6 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
     }
     uint4* my_x = xch + (size_t)yy0 * SXp + sx;  // row q at + q * SXp
     const size_t plane_stride = (size_t)Y * SX;
-    const size_t xpar = (size_t)rows * SXp;
 
     int zo = zfirst + zstep;
     // Fetch f is the (f / kRing)-th use of slot f % kRing, so the phase parity to wait for is
@@ -208,7 +225,7 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
         if (!mbar_wait_bounded(&bars[s], (uint32_t)(f >> kRingLog2) & 1u, kWaitLimitNs)) err = kErrWaitTimeout;
 #pragma unroll
         for (int q = 0; q < kStrips; q++)
-            out[q] = has[q] ? my_ring[(size_t)s * slot_stride + (size_t)q * SX] : make_uint4(0, 0, 0, 0);
+            out[q] = has[q] && ring_ok(s, q) ? my_ring[(size_t)s * slot_stride + (size_t)q * SX] : make_uint4(0, 0, 0, 0);
     };
     Row r_m[kStrips], r_c[kStrips];
     uint4 s_c[kStrips];
@@ -237,7 +254,8 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
             if (!mbar_wait_bounded(&bars[s], (uint32_t)(f >> kRingLog2) & 1u, kWaitLimitNs)) err = kErrWaitTimeout;
 #pragma unroll
             for (int q = 0; q < kStrips; q++)
-                s_in[q] = (kDense || has[q]) ? my_ring[(size_t)s * slot_stride + (size_t)q * SX] : make_uint4(0, 0, 0, 0);
+                s_in[q] = (kDense || has[q]) && ring_ok(s, q) ? my_ring[(size_t)s * slot_stride + (size_t)q * SX]
+                                                              : make_uint4(0, 0, 0, 0);
         }
         Row r_p[kStrips];
         uint32_t pc[kStrips][P::NC], ps[kStrips][P::NS];
@@ -247,8 +265,10 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
             P::make(r_m[q], r_c[q], r_p[q], pc[q], ps[q]);
         }
         uint4* xb = my_x + (size_t)(U & 1) * xpar;
-        xb[0] = pack_planes<P::NS>(ps[0]);
-        if constexpr (kStrips > 1) xb[(size_t)(kStrips - 1) * SXp] = pack_planes<P::NS>(ps[kStrips - 1]);
+        const size_t xb_rel = (size_t)(U & 1) * xpar;
+        if (x_ok(xb_rel)) xb[0] = pack_planes<P::NS>(ps[0]);
+        if constexpr (kStrips > 1)
+            if (x_ok(xb_rel + (size_t)(kStrips - 1) * SXp)) xb[(size_t)(kStrips - 1) * SXp] = pack_planes<P::NS>(ps[kStrips - 1]);
         __syncthreads();
         if (threadIdx.x == producer) {
             fence_proxy_async();
@@ -259,14 +279,15 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
             if (outp[q]) {
                 uint32_t psm[4], psp[4];
                 if (q == 0) {
-                    const uint4 t = *(xb - SXp);
+                    const uint4 t = x_ok(xb_rel - SXp) ? *(xb - SXp) : make_uint4(0, 0, 0, 0);
                     psm[0] = t.x; psm[1] = t.y; psm[2] = t.z; psm[3] = t.w;
                 } else {
 #pragma unroll
                     for (int i = 0; i < P::NS; i++) psm[i] = ps[q - 1][i];
                 }
                 if (q == kStrips - 1) {
-                    const uint4 t = *(xb + (size_t)kStrips * SXp);
+                    const uint4 t = x_ok(xb_rel + (size_t)kStrips * SXp) ? *(xb + (size_t)kStrips * SXp)
+                                                                          : make_uint4(0, 0, 0, 0);
                     psp[0] = t.x; psp[1] = t.y; psp[2] = t.z; psp[3] = t.w;
                 } else {
 #pragma unroll
@@ -274,9 +295,10 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
                 }
                 uint32_t cnt[count_bits(NB)];
                 P::combine(pc[q], psm, psp, cnt);
-                my_dst[q][(size_t)zo * plane_stride] =
-                    update_strip<NB, NT, kCountZero, Fixed::kFullRange, kPop>(s_c[q], r_c[q].a, cnt, valid, R, acc,
-                                                                                xbits[q], (uint32_t)zo);
+                const uint4 n = update_strip<NB, NT, kCountZero, Fixed::kFullRange, kPop>(
+                    s_c[q], r_c[q].a, cnt, valid, R, acc, xbits[q], (uint32_t)zo);
+                if (CAVE_IN_BOUNDS((size_t)max(y[q], 0) * SX + sx + (size_t)zo * plane_stride, copy_n, err))
+                    my_dst[q][(size_t)zo * plane_stride] = n;
             }
         }
 #pragma unroll
@@ -315,17 +337,17 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
         bx0 = sx * 32u + (uint32_t)(__ffs(xall) - 1);
         bx1 = sx * 32u + 31u - (uint32_t)__clz(xall);
     }
-    uint32_t v[11] = {acc.surviving, acc.born, acc.zero, acc.population, bx0, by0, acc.zmin, bx1, by1, acc.zmax, err};
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-        for (int q = 0; q < 4; q++) v[q] += __shfl_xor_sync(0xFFFFFFFFu, v[q], o);
-#pragma unroll
-        for (int q = 4; q < 7; q++) v[q] = min(v[q], __shfl_xor_sync(0xFFFFFFFFu, v[q], o));
-#pragma unroll
-        for (int q = 7; q < 10; q++) v[q] = max(v[q], __shfl_xor_sync(0xFFFFFFFFu, v[q], o));
-        v[10] |= __shfl_xor_sync(0xFFFFFFFFu, v[10], o);
+    bool slots_ok = true;
+#ifdef CAVE_CHECKED
+    if (tick_arg >= 0) {  // the deferred-fold slots this launch adds to: tick, and tick - 1 for kPopInput
+        const uint32_t tick_limit = sim->tick_limit;
+        slots_ok = CAVE_IN_BOUNDS(tick, tick_limit, err) &&
+                   (kPop != kPopInput || CAVE_IN_BOUNDS(tick - 1u, tick_limit, err));
     }
+#endif
+    uint32_t v[11] = {acc.surviving, acc.born, acc.zero, acc.population, bx0, by0, acc.zmin, bx1, by1, acc.zmax, err};
+    warp_reduce_tick(v);
+    v[10] = warp_or(v[10]);
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     if (lane == 0) {
 #pragma unroll
@@ -351,6 +373,10 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
     if (tick_arg >= 0) {
         // deferred fold: add this CTA's totals to the tick's slot (no ticket, no fence: the next
         // launch starts after this one has completed and flushed)
+        if (!slots_ok) {  // checked build: only the error flags are applied
+            if (lane == 10u && x) atomicOr(&sim->error, x);
+            return;
+        }
         TickTotals* d = sim->deferred + tick;
         TickTotals* dp = kPop == kPopInput ? d - 1 : d;  // the slot the population belongs to
         if (lane < 3u && x) atomicAdd(&d->surv + lane, x);

@@ -42,10 +42,54 @@ __host__ __device__ inline size_t stream2_smem_bytes(uint32_t rows, uint32_t SX,
 // kFirst: the run's first launch (ticks 0 and 1). kDense: the launch guarantees SX == SXp.
 // kStrips: rows per thread. src_sel: the cell copy (0 / 1) holding the input; the output goes to
 // the other one.
-template <int NB, class Fixed, bool kFirst, bool kDense, int kStrips>
+// kChain: the launch runs `npasses` two-tick passes (ticks tick_arg + 2p, + 2p + 1, reading copy
+// src_sel ^ (p & 1)) instead of one. It must be a cooperative launch of one CTA per item, the
+// items laid out z-major with `chain_ny` items per z-row and every tile at least two rows high
+// and every slab at least two planes deep except the last ones: a pass reads the previous
+// pass's output in its tile and the two rows / planes around it, which only the eight
+// neighbouring items write. Before pass p > 0 a CTA waits until each neighbour's flag
+// (chain_flags[item], zeroed before the launch) reads p, i.e. the neighbour has written its part
+// of pass p - 1 and no longer reads the copy pass p overwrites; after each pass it publishes its
+// own. The waits are bounded: a CTA that gives up (or sees a neighbour that gave up) marks its
+// flag as aborted, raises kErrWaitTimeout and stops.
+constexpr uint32_t kChainAbort = 0xFFFFFFFFu;
+
+// Waits (one thread) until every neighbour of item i in the ny-wide item grid has published
+// `need`; 0 when they have, 1 after kWaitLimitNs, 2 when a neighbour aborted.
+__device__ __forceinline__ uint32_t chain_wait(const uint32_t* flags, uint32_t i, uint32_t ny, uint32_t n,
+                                               uint32_t need) {
+    const int iy = (int)(i % ny), iz = (int)(i / ny), nz = (int)(n / ny);
+    uint64_t t0 = 0;
+    for (bool first = true;; first = false) {
+        bool ready = true, aborted = false;
+#pragma unroll
+        for (int dz = -1; dz <= 1; dz++) {
+#pragma unroll
+            for (int dy = -1; dy <= 1; dy++) {
+                const int jy = iy + dy, jz = iz + dz;
+                if ((dy == 0 && dz == 0) || jy < 0 || jy >= (int)ny || jz < 0 || jz >= nz) continue;
+                const uint32_t v = ld_acquire_gpu(flags + (size_t)jz * ny + jy);
+                aborted |= v == kChainAbort;
+                ready &= v >= need;
+            }
+        }
+        if (aborted) return 2;
+        if (ready) return 0;
+        if (first) {
+            t0 = global_ns();
+        } else if (global_ns() - t0 > kWaitLimitNs) {
+            return 1;
+        }
+    }
+}
+
+template <int NB, class Fixed, bool kFirst, bool kDense, int kStrips, bool kChain = false>
 __device__ __forceinline__ void stream_tick2_body(const StreamItem* __restrict__ items, StripSim* sims, uint4* pool,
-                                                  uint32_t sxp_log2, int tick_arg, int src_sel) {
+                                                  uint32_t sxp_log2, int tick_arg, int src_sel, uint32_t npasses = 1,
+                                                  uint32_t* chain_flags = nullptr, uint32_t chain_ny = 1) {
     static_assert(Fixed::kFixed, "the two-tick kernel is compiled for one rule");
+    static_assert(!(kChain && kFirst), "a chained launch follows the run's first pair");
+    __shared__ uint32_t s_abort;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ uint32_t red[32][21];
     const StreamItem it = items[blockIdx.x];
@@ -67,21 +111,17 @@ __device__ __forceinline__ void stream_tick2_body(const StreamItem* __restrict__
     __syncthreads();
     // Everything below reads the previous launch's results.
     asm volatile("griddepcontrol.wait;" ::: "memory");
-    const uint32_t tick = (uint32_t)tick_arg;
     asm volatile("griddepcontrol.launch_dependents;");
-    const uint4* src = reinterpret_cast<const uint4*>(reinterpret_cast<unsigned char*>(pool) + (src_sel ? buf1 : buf0));
-    uint4* dst = reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(pool) + (src_sel ? buf0 : buf1));
 
     const uint32_t sx = threadIdx.x & (SXp - 1u), yy0 = kStrips * (threadIdx.x >> sxp_log2);
     const uint32_t ty = it.ty;
     int y[kStrips];
-    bool has[kStrips], rowA[kStrips], own[kStrips];
+    bool has[kStrips], own[kStrips];
 #pragma unroll
     for (int q = 0; q < kStrips; q++) {
         const uint32_t yy = yy0 + q;
         y[q] = (int)it.y0 - 2 + (int)yy;
         has[q] = sx < SX && y[q] >= 0 && y[q] < (int)Y && yy < ty + 4u;
-        rowA[q] = has[q] && yy >= 1 && yy <= ty + 2u;  // stage A computes this row
         own[q] = has[q] && yy >= 2 && yy <= ty + 1u;   // stage B computes it; both count it
     }
     const uint32_t valid = sx < SX ? strip_valid(sx, X) : 0u;
@@ -99,6 +139,49 @@ __device__ __forceinline__ void stream_tick2_body(const StreamItem* __restrict__
     const bool down = (it.dir_items & 1u) != 0;
     const int zstep = down ? -1 : 1;
     const int zfirst = down ? (int)it.z1 + 1 : (int)it.z0 - 2;  // plane of fetch 0
+    uint32_t err = 0;
+    // extents (uint4 units) that the checked build tests every index against; a layout that does
+    // not fit the launch's shared memory fails every shared-memory check
+    const size_t xpar = (size_t)rows * SXp;
+    size_t ring_n = (size_t)kRing * slot_stride, xch_n = (size_t)2 * kXch * xpar;
+    const size_t copy_n = (size_t)Z * Y * SX;
+#ifdef CAVE_CHECKED
+    if (!CAVE_IN_BOUNDS((ring_n + xch_n) * 16 + kRing * 8 - 1, dynamic_smem_bytes(), err)) ring_n = xch_n = 0;
+    const uint32_t tick_limit = sim->tick_limit;
+#endif
+    const size_t ring_off = (size_t)yy0 * SX + sx, x_off = (size_t)yy0 * SXp + sx;
+
+  for (uint32_t pass = 0; pass < npasses; pass++) {
+    const uint32_t tick = (uint32_t)tick_arg + 2u * pass;
+    const int sel = src_sel ^ (int)(pass & 1u);
+    const uint4* src = reinterpret_cast<const uint4*>(reinterpret_cast<unsigned char*>(pool) + (sel ? buf1 : buf0));
+    uint4* dst = reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(pool) + (sel ? buf0 : buf1));
+    if constexpr (kChain) {
+        if (pass > 0) {
+            // the neighbours' part of the previous pass; then fresh ring barriers (no copy is in
+            // flight: every fetch of the previous pass was waited for)
+            if (threadIdx.x == 0) {
+                const uint32_t w = chain_wait(chain_flags, blockIdx.x, chain_ny, gridDim.x, pass);
+                s_abort = w;
+                if (w == 0) {
+                    fence_proxy_async_all();  // the copies below read what the generic stores wrote
+                    for (int q = 0; q < kRing; q++) {
+                        mbar_inval(&bars[q]);
+                        mbar_init(&bars[q], 1);
+                    }
+                    mbar_init_fence();
+                }
+            }
+            __syncthreads();
+            if (s_abort) {
+                if (threadIdx.x == 0) {
+                    st_release_gpu(chain_flags + blockIdx.x, kChainAbort);
+                    atomicOr(&sim->error, kErrWaitTimeout);
+                }
+                break;
+            }
+        }
+    }
 
     // Thread 0 fills ring slot f % kRing with input plane f; a plane outside the grid completes
     // its slot's phase with a plain arrive (every fetch advances its slot by one phase).
@@ -110,26 +193,30 @@ __device__ __forceinline__ void stream_tick2_body(const StreamItem* __restrict__
             mbar_arrive(&bars[s]);
             return;
         }
-        uint4* slot = ring + (size_t)s * slot_stride + (size_t)slot_row0 * SX;
-        const uint4* g = src + ((size_t)p * Y + (size_t)ylo) * SX;
+        const size_t slot_i = (size_t)s * slot_stride + (size_t)slot_row0 * SX, g_i = ((size_t)p * Y + (size_t)ylo) * SX;
+        if (!CAVE_IN_BOUNDS(slot_i + tile_bytes / 16u - 1u, ring_n, err) ||
+            !CAVE_IN_BOUNDS(g_i + tile_bytes / 16u - 1u, copy_n, err)) {
+            mbar_arrive(&bars[s]);  // checked build: the copy is skipped, its phase completed
+            return;
+        }
         mbar_expect_tx(&bars[s], tile_bytes);
-        bulk_g2s(slot, g, tile_bytes, &bars[s]);
+        bulk_g2s(ring + slot_i, src + g_i, tile_bytes, &bars[s]);
     };
     if (threadIdx.x == 0) {
         for (int f = 0; f < kRing; f++) issue(f);
     }
     const uint4* my_ring = ring + (size_t)yy0 * SX + sx;  // row q at + q * SX
-    if constexpr (kDense) {
+    if (kDense && pass == 0) {
 #pragma unroll
         for (int q = 0; q < kStrips; q++) {
             if (!has[q]) {
 #pragma unroll
                 for (int s = 0; s < kRing; s++)
-                    const_cast<uint4*>(my_ring)[(size_t)s * slot_stride + (size_t)q * SX] = make_uint4(0, 0, 0, 0);
+                    if (CAVE_IN_BOUNDS(ring_off + (size_t)s * slot_stride + (size_t)q * SX, ring_n, err))
+                        const_cast<uint4*>(my_ring)[(size_t)s * slot_stride + (size_t)q * SX] = make_uint4(0, 0, 0, 0);
             }
         }
     }
-    uint32_t err = 0;
     auto row_of = [&](uint4 st) -> Row {
         const uint32_t a = alive_plane(st, R);
         const uint32_t v = a & send_mask;
@@ -150,7 +237,10 @@ __device__ __forceinline__ void stream_tick2_body(const StreamItem* __restrict__
         if (!mbar_wait_bounded(&bars[s], (uint32_t)(f >> kRingLog2) & 1u, kWaitLimitNs)) err = kErrWaitTimeout;
 #pragma unroll
         for (int q = 0; q < kStrips; q++)
-            out[q] = (kDense || has[q]) ? my_ring[(size_t)s * slot_stride + (size_t)q * SX] : make_uint4(0, 0, 0, 0);
+            out[q] = (kDense || has[q]) &&
+                             CAVE_IN_BOUNDS(ring_off + (size_t)s * slot_stride + (size_t)q * SX, ring_n, err)
+                         ? my_ring[(size_t)s * slot_stride + (size_t)q * SX]
+                         : make_uint4(0, 0, 0, 0);
     };
 
     using P = typename ColumnsFor<NB, true>::type;
@@ -158,18 +248,23 @@ __device__ __forceinline__ void stream_tick2_body(const StreamItem* __restrict__
     accA.reset(SX != 0u ? 1u : 0u);  // SX >= 1: a 1 the compiler cannot fold (see mad_add)
     accB.reset(accA.one);
     uint32_t xbA[kStrips], xbB[kStrips];
-    uint4* my_dst[kStrips];
+    // strip index of each row in a plane of the output copy (a copy holds at most 2^25 strips),
+    // and stage A's valid mask per row: 0 on rows outside the grid, whose input is all 0, so
+    // that their stage-A result is 0 (outside the grid is dead) without a select
+    uint32_t dst_row[kStrips], validA[kStrips];
 #pragma unroll
     for (int q = 0; q < kStrips; q++) {
         xbA[q] = xbB[q] = 0u;
-        my_dst[q] = dst + ((size_t)max(y[q], 0) * SX + sx);
+        dst_row[q] = (uint32_t)max(y[q], 0) * SX + sx;
+        validA[q] = has[q] ? valid : 0u;
     }
+    const uint32_t plane_strips = Y * SX;
     uint4* my_x = xch + (size_t)yy0 * SXp + sx;  // row q at + q * SXp; stage B at + kXch * xpar
     // offsets of the rows above and below this thread's rows in an exchange buffer, clamped to
     // its own row at the tile's first and last thread rows (whose results are not used)
     const size_t x_dn = yy0 > 0 ? (size_t)SXp : 0, x_up = yy0 + kStrips < rows ? (size_t)kStrips * SXp : 0;
-    const size_t plane_stride = (size_t)Y * SX;
-    const size_t xpar = (size_t)rows * SXp;
+    // the checked build's test of an exchange-buffer index, relative to my_x
+    auto x_ok = [&](size_t rel) { return CAVE_IN_BOUNDS(x_off + rel, xch_n, err); };
 
     // rolling state: stage A input rows (planes f-2, f-1) and centre state; stage A outputs
     // A(f-2), A(f-3); stage B rows of A(f-4), A(f-3)
@@ -212,8 +307,11 @@ __device__ __forceinline__ void stream_tick2_body(const StreamItem* __restrict__
                 rAp[q] = row_of(s_in[q]);
                 P::make(rAm[q], rAc[q], rAp[q], pcA[q], psA[q]);
             }
-            xa[0] = pack_planes<P::NS>(psA[0]);
-            if constexpr (kStrips > 1) xa[(size_t)(kStrips - 1) * SXp] = pack_planes<P::NS>(psA[kStrips - 1]);
+            const size_t xa_rel = (size_t)(U & 1) * xpar;
+            if (x_ok(xa_rel)) xa[0] = pack_planes<P::NS>(psA[0]);
+            if constexpr (kStrips > 1)
+                if (x_ok(xa_rel + (size_t)(kStrips - 1) * SXp))
+                    xa[(size_t)(kStrips - 1) * SXp] = pack_planes<P::NS>(psA[kStrips - 1]);
         }
         // ---- stage B: rows of A(f-2)
         Row rBp[kStrips];
@@ -223,36 +321,41 @@ __device__ __forceinline__ void stream_tick2_body(const StreamItem* __restrict__
         if (actB) {
 #pragma unroll
             for (int q = 0; q < kStrips; q++) P::make(rBm[q], rBc[q], rBp[q], pcB[q], psB[q]);
-            xb[0] = pack_planes<P::NS>(psB[0]);
-            if constexpr (kStrips > 1) xb[(size_t)(kStrips - 1) * SXp] = pack_planes<P::NS>(psB[kStrips - 1]);
+            const size_t xb_rel = (size_t)(U & 1) * xpar + (size_t)kXch * xpar;
+            if (x_ok(xb_rel)) xb[0] = pack_planes<P::NS>(psB[0]);
+            if constexpr (kStrips > 1)
+                if (x_ok(xb_rel + (size_t)(kStrips - 1) * SXp))
+                    xb[(size_t)(kStrips - 1) * SXp] = pack_planes<P::NS>(psB[kStrips - 1]);
         }
         __syncthreads();
         if (threadIdx.x == 0) {
             fence_proxy_async();
             issue(f + kRing);
         }
-        // ---- stage A: A(f - 1), plane zA. Every row is computed and rows stage A does not own
-        // are masked to 0 afterwards (a branch per row would split the step into blocks the
-        // compiler cannot interleave); the neighbour-row reads of edge rows are clamped in-bounds
-        // and their results discarded.
+        // ---- stage A: A(f - 1), plane zA. Every row is computed, branch-free (a branch per row
+        // would split the step into blocks the compiler cannot interleave). Rows and planes
+        // outside the grid have input 0 and valid mask 0, so their result is 0. The tile's two
+        // outermost rows (0 and ty + 3) read clamped neighbour rows and come out wrong; they feed
+        // only stage B's rows 1 and ty + 2, which are neither stored nor counted.
         uint4 nA1[kStrips];
         if (actA) {
             const int jA = f - 1;
             const int zA = zfirst + jA * zstep;
             const bool inA = !checked || (unsigned)zA < Z;
             const bool ownA = !checked || (jA >= 2 && jA <= L + 1);
+            uint32_t zany = 0u;
 #pragma unroll
             for (int q = 0; q < kStrips; q++) {
                 uint32_t psm[4], psp[4];
                 if (q == 0) {
-                    const uint4 t = *(xa - x_dn);
+                    const uint4 t = x_ok((size_t)(U & 1) * xpar - x_dn) ? *(xa - x_dn) : make_uint4(0, 0, 0, 0);
                     psm[0] = t.x; psm[1] = t.y; psm[2] = t.z; psm[3] = t.w;
                 } else {
 #pragma unroll
                     for (int i = 0; i < P::NS; i++) psm[i] = psA[q - 1][i];
                 }
                 if (q == kStrips - 1) {
-                    const uint4 t = *(xa + x_up);
+                    const uint4 t = x_ok((size_t)(U & 1) * xpar + x_up) ? *(xa + x_up) : make_uint4(0, 0, 0, 0);
                     psp[0] = t.x; psp[1] = t.y; psp[2] = t.z; psp[3] = t.w;
                 } else {
 #pragma unroll
@@ -260,28 +363,34 @@ __device__ __forceinline__ void stream_tick2_body(const StreamItem* __restrict__
                 }
                 uint32_t cnt[count_bits(NB)];
                 P::combine(pcA[q], psm, psp, cnt);
-                const uint4 n = update_strip<NB, 0, kFirst, Fixed::kFullRange, kFirst ? kPopNone : kPopInput>(
-                    sAc[q], rAc[q].a, cnt, valid, R, accA, xbA[q], (uint32_t)zA, own[q] && ownA);
-                const bool keep = rowA[q] && inA;
-                nA1[q] = keep ? n : make_uint4(0, 0, 0, 0);
+                nA1[q] = update_strip<NB, 0, kFirst, Fixed::kFullRange, kFirst ? kPopNone : kPopInput, false>(
+                    sAc[q], rAc[q].a, cnt, inA ? validA[q] : 0u, R, accA, xbA[q], (uint32_t)zA, own[q] && ownA,
+                    &zany);
+            }
+            if (zany) {
+                accA.zmin = min(accA.zmin, (uint32_t)zA);
+                accA.zmax = max(accA.zmax, (uint32_t)zA);
             }
         }
         // ---- stage B: B(f - 3), plane zB, written to HBM (rows it owns; the others computed and
         // dropped, as in stage A)
         if (actB) {
             const int zB = zfirst + (f - 3) * zstep;
+            uint32_t zany = 0u;
 #pragma unroll
             for (int q = 0; q < kStrips; q++) {
                 uint32_t psm[4], psp[4];
                 if (q == 0) {
-                    const uint4 t = *(xb - x_dn);
+                    const uint4 t = x_ok((size_t)((U & 1) + kXch) * xpar - x_dn) ? *(xb - x_dn)
+                                                                                   : make_uint4(0, 0, 0, 0);
                     psm[0] = t.x; psm[1] = t.y; psm[2] = t.z; psm[3] = t.w;
                 } else {
 #pragma unroll
                     for (int i = 0; i < P::NS; i++) psm[i] = psB[q - 1][i];
                 }
                 if (q == kStrips - 1) {
-                    const uint4 t = *(xb + x_up);
+                    const uint4 t = x_ok((size_t)((U & 1) + kXch) * xpar + x_up) ? *(xb + x_up)
+                                                                                   : make_uint4(0, 0, 0, 0);
                     psp[0] = t.x; psp[1] = t.y; psp[2] = t.z; psp[3] = t.w;
                 } else {
 #pragma unroll
@@ -289,9 +398,14 @@ __device__ __forceinline__ void stream_tick2_body(const StreamItem* __restrict__
                 }
                 uint32_t cnt[count_bits(NB)];
                 P::combine(pcB[q], psm, psp, cnt);
-                const uint4 n = update_strip<NB, 0, false, Fixed::kFullRange, kPopInput>(
-                    nA3[q], rBc[q].a, cnt, valid, R, accB, xbB[q], (uint32_t)zB, own[q]);
-                if (own[q]) my_dst[q][(size_t)zB * plane_stride] = n;
+                const uint4 n = update_strip<NB, 0, false, Fixed::kFullRange, kPopInput, false>(
+                    nA3[q], rBc[q].a, cnt, valid, R, accB, xbB[q], (uint32_t)zB, own[q], &zany);
+                const uint32_t di = (uint32_t)zB * plane_strips + dst_row[q];
+                if (own[q] && CAVE_IN_BOUNDS(di, copy_n, err)) dst[di] = n;
+            }
+            if (zany) {
+                accB.zmin = min(accB.zmin, (uint32_t)zB);
+                accB.zmax = max(accB.zmax, (uint32_t)zB);
             }
         }
         // ---- rotate
@@ -324,6 +438,7 @@ __device__ __forceinline__ void stream_tick2_body(const StreamItem* __restrict__
 
     // ---- per-CTA reduction of both ticks' statistics
     uint32_t v[21];
+    bool slots_ok = true;
     {
         uint32_t ax0 = 0xFFFFFFFFu, ax1 = 0u, ay0 = 0xFFFFFFFFu, ay1 = 0u, xa = 0u;
         uint32_t bx0 = 0xFFFFFFFFu, bx1 = 0u, by0 = 0xFFFFFFFFu, by1 = 0u, xb = 0u;
@@ -348,6 +463,11 @@ __device__ __forceinline__ void stream_tick2_body(const StreamItem* __restrict__
             bx0 = sx * 32u + (uint32_t)(__ffs(xb) - 1);
             bx1 = sx * 32u + 31u - (uint32_t)__clz(xb);
         }
+#ifdef CAVE_CHECKED
+        // the statistics slots: stage A's input population goes to slot tick - 1 (none for the
+        // run's first launch), stage B's to slot tick + 1
+        slots_ok = CAVE_IN_BOUNDS(tick + 1u, tick_limit, err) && (kFirst || CAVE_IN_BOUNDS(tick - 1u, tick_limit, err));
+#endif
         const uint32_t vv[21] = {accA.surviving, accA.born, accA.zero, accA.population, ax0, ay0, accA.zmin,
                                  ax1, ay1, accA.zmax,
                                  accB.surviving, accB.born, accB.zero, accB.population, bx0, by0, accB.zmin,
@@ -355,26 +475,16 @@ __device__ __forceinline__ void stream_tick2_body(const StreamItem* __restrict__
 #pragma unroll
         for (int q = 0; q < 21; q++) v[q] = vv[q];
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-#pragma unroll
-            for (int q = 0; q < 4; q++) v[10 * h + q] += __shfl_xor_sync(0xFFFFFFFFu, v[10 * h + q], o);
-#pragma unroll
-            for (int q = 4; q < 7; q++) v[10 * h + q] = min(v[10 * h + q], __shfl_xor_sync(0xFFFFFFFFu, v[10 * h + q], o));
-#pragma unroll
-            for (int q = 7; q < 10; q++) v[10 * h + q] = max(v[10 * h + q], __shfl_xor_sync(0xFFFFFFFFu, v[10 * h + q], o));
-        }
-        v[20] |= __shfl_xor_sync(0xFFFFFFFFu, v[20], o);
-    }
+    warp_reduce_tick(v);
+    warp_reduce_tick(v + 10);
+    v[20] = warp_or(v[20]);
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     if (lane == 0) {
 #pragma unroll
         for (int q = 0; q < 21; q++) red[warp][q] = v[q];
     }
     __syncthreads();
-    if (warp != 0) return;
+    if (warp == 0) {
     if (lane == 0) {
         const uint32_t nw = blockDim.x >> 5;
         for (uint32_t w = 1; w < nw; w++) {
@@ -390,6 +500,7 @@ __device__ __forceinline__ void stream_tick2_body(const StreamItem* __restrict__
     // lane q applies column q: stage A (tick) 0..9, stage B (tick + 1) 10..19, error flags 20
     const uint32_t x = red[0][lane < 21u ? lane : 20u];
     const uint32_t popA = __shfl_sync(0xFFFFFFFFu, x, 3), popB = __shfl_sync(0xFFFFFFFFu, x, 13);
+    if (slots_ok || lane >= 20u) {  // checked build: only the error flags when a slot is out of range
     TickTotals* dA = deferred + tick;  // stage A's slot; its input's population goes to dA - 1
     TickTotals* dB = dA + 1;           // stage B's slot; its input's population goes to dA
     if (lane < 3u) {
@@ -411,6 +522,15 @@ __device__ __forceinline__ void stream_tick2_body(const StreamItem* __restrict__
     } else if (lane == 20u) {
         if (x) atomicOr(&sim->error, x);
     }
+    }
+    }
+    if constexpr (kChain) {
+        // publish this pass: every thread's stores visible GPU-wide, then the flag
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) st_release_gpu(chain_flags + blockIdx.x, pass + 1u);
+    }
+  }  // passes
 }
 
 }  // namespace cave

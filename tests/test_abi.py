@@ -31,14 +31,19 @@ def test_library_builds_and_loads():
     cb.lib()
 
 
-def test_every_declared_symbol_is_exported():
+CHECKED_LIB = os.path.join(ROOT, "cave_b200", "libcave_ca_checked.so")
+
+
+@pytest.mark.parametrize("path", [cb.LIB_PATH, CHECKED_LIB], ids=["library", "checked-library"])
+def test_every_declared_symbol_is_exported(path):
+    assert os.path.exists(path), "run python -m cave_b200.build (--checked for the checked library)"
     decl = declared_functions()
     assert len(decl) >= 15
-    out = subprocess.run(["nm", "-D", "--defined-only", cb.LIB_PATH], capture_output=True, text=True).stdout
+    out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True).stdout
     exported = {line.split()[-1] for line in out.splitlines() if " T " in line}
     missing = decl - exported
     assert not missing, f"declared but not exported: {sorted(missing)}"
-    L = ctypes.CDLL(cb.LIB_PATH)
+    L = ctypes.CDLL(path)
     for n in decl:
         getattr(L, n)
 

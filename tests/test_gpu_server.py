@@ -188,9 +188,9 @@ def test_cancel_unknown_request_is_an_error(ctx):
 
 
 def long_request(n, edge=256, ticks=300):
-    """n copies of a simulation that stays alive for all its ticks (Moore S{3,4} B{4}, C = 16)."""
+    """n copies of a simulation that stays alive for all its ticks (Moore S{4,5} B{5}, C = 16)."""
     r = cb.request_sims(n)
-    p = O.make_params(16, 0x7, 1 << 4, (1 << 3) | (1 << 4))
+    p = O.make_params(15, 0x7, 1 << 4, (1 << 3) | (1 << 4))
     for i in range(n):
         r[i]["X"] = r[i]["Y"] = r[i]["Z"] = edge
         r[i]["maxTicks"] = ticks
@@ -210,7 +210,7 @@ def test_request_deadline_expires_and_later_requests_run(ctx):
     rng = np.random.default_rng(43)
     small = make_request(rng, 4, edges=(24, 33))
     alone = run_alone(ctx, small, hbm_budget=1 << 30)
-    big = long_request(200)  # one at a time: seconds of work
+    big = long_request(400)  # one simulation at a time, one tick per round: seconds of work
     with cb.Server(ctx, hbm_budget=1 << 30, max_active_cells=1, ticks_per_round=1, request_deadline=1.0) as s:
         t0 = time.time()
         rid = s.submit(big)
