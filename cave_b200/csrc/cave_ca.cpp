@@ -548,17 +548,6 @@ static bool pair_ticks_enabled() {
     return !(v && (!std::strcmp(v, "0") || !std::strcmp(v, "off")));
 }
 
-// After the run's first pair, the remaining pairs run as passes of one cooperative launch (the
-// chain kernels) when the plan allows it: tiles at least two rows high and slabs at least two
-// planes deep (a pass's halo then lies in the neighbouring items only). Only with
-// CAVE_TICK2_CHAIN=1 for now; otherwise one launch per pair.
-static bool chain_enabled(const StreamPlan& plan) {
-    const char* v = std::getenv("CAVE_TICK2_CHAIN");
-    if (!v || std::strcmp(v, "1")) return false;
-    if (plan.items.empty()) return false;
-    const StreamItem& it = plan.items[0];
-    return (plan.ny == 1 || it.ty >= 2) && (plan.nz == 1 || it.z1 - it.z0 >= 2);
-}
 
 static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* host_out, const cave_sim_params* params,
                             const uint64_t* validBitmasks, uint32_t nValid, uint32_t maxRuleBits, uint32_t nticks,
@@ -696,9 +685,7 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
     if (e == cudaSuccess && lead && !run_plan(ctx, g, 0, kRunJit, cps, env_cps != nullptr, plan1))
         return set_error(ctx, CAVE_ERR_INTERNAL, "streaming plan failed");
     const size_t n_main = plan.items.size(), n_lead = lead ? plan1.items.size() : 0;
-    // the items of both plans, then one flag word per main item (the chain kernels' pass flags)
-    if (e == cudaSuccess) e = cudaMalloc(&ditems, sizeof(StreamItem) * (n_main + n_lead) + sizeof(uint32_t) * n_main);
-    uint32_t* chain_flags = e == cudaSuccess ? reinterpret_cast<uint32_t*>(ditems + n_main + n_lead) : nullptr;
+    if (e == cudaSuccess) e = cudaMalloc(&ditems, sizeof(StreamItem) * (n_main + n_lead));
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(ditems, plan.items.data(), sizeof(StreamItem) * n_main, cudaMemcpyHostToDevice,
                             ctx->stream);
@@ -722,29 +709,8 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
             sel = 1;
             launches++;
         }
-        const bool dense = plan.SX == plan.SXp;
-        bool chain = jk.chain[dense] && chain_enabled(plan);
-        while (t + 1 < nticks && e == cudaSuccess) {
-            const uint32_t passes = (nticks - t) / 2;
-            if (chain && t > 0 && passes >= 2) {
-                e = cudaMemsetAsync(chain_flags, 0, sizeof(uint32_t) * n_main, ctx->stream);
-                if (e == cudaSuccess)
-                    e = launch_stream_tick2_chain_jit(jk.chain[dense], ditems, (uint32_t)n_main, g->sim, g->strips,
-                                                      plan.SX, plan.SXp, plan.threads, ctx->stream, (int)t, (int)sel,
-                                                      passes, chain_flags, plan.ny);
-                if (e == cudaErrorCooperativeLaunchTooLarge) {  // the items do not fit at once: a launch per pair
-                    (void)cudaGetLastError();
-                    e = cudaSuccess;
-                    chain = false;
-                    continue;
-                }
-                t += 2 * passes;
-                sel ^= passes & 1u;
-                launches++;
-                continue;
-            }
+        for (; t + 1 < nticks && e == cudaSuccess; t += 2) {
             e = launch_run_tick(ctx, g, kind, s.rule, jk, plan, ditems, t == 0, true, t, sel);
-            t += 2;
             sel ^= 1u;
             launches++;
         }

@@ -80,21 +80,11 @@ CAVE_JIT_KERNEL2(cave_stream_tick2_jit_first, true, false)
 CAVE_JIT_KERNEL2(cave_stream_tick2_jit, false, false)
 CAVE_JIT_KERNEL2(cave_stream_tick2_jit_dense_first, true, true)
 CAVE_JIT_KERNEL2(cave_stream_tick2_jit_dense, false, true)
-#define CAVE_JIT_KERNEL2C(NAME, DENSE)                                                                     \
-    extern "C" __global__ void __launch_bounds__(cave::kJit2MaxThreads, cave::kJit2CtasPerSm)              \
-        NAME(const cave::StreamItem* __restrict__ items, cave::StripSim* sims, uint4* pool, uint32_t sxp_log2, \
-             int tick_arg, int src_sel, uint32_t npasses, uint32_t* flags, uint32_t ny) {                  \
-        cave::stream_tick2_body<CAVE_JIT_NB, cave::JitRule, false, DENSE, cave::kJit2RowsPerThread, true>( \
-            items, sims, pool, sxp_log2, tick_arg, src_sel, npasses, flags, ny);                           \
-    }
-CAVE_JIT_KERNEL2C(cave_stream_tick2_jit_chain, false)
-CAVE_JIT_KERNEL2C(cave_stream_tick2_jit_dense_chain, true)
 )cave_unit";
 const char* const kJitCounting[2] = {"cave_stream_tick_jit", "cave_stream_tick_jit_dense"};
 const char* const kJitDerived[2] = {"cave_stream_tick_jit_derived", "cave_stream_tick_jit_dense_derived"};
 const char* const kJitPairFirst[2] = {"cave_stream_tick2_jit_first", "cave_stream_tick2_jit_dense_first"};
 const char* const kJitPair[2] = {"cave_stream_tick2_jit", "cave_stream_tick2_jit_dense"};
-const char* const kJitChain[2] = {"cave_stream_tick2_jit_chain", "cave_stream_tick2_jit_dense_chain"};
 
 struct Nvrtc {
     bool ok = false;
@@ -441,7 +431,6 @@ JitKernels jit_stream_kernel(const JitKey& k, JitMode mode, bool start) {
         if (err == cudaSuccess) err = cudaLibraryGetKernel(&e->kern.derived[d], e->lib, kJitDerived[d]);
         if (err == cudaSuccess) err = cudaLibraryGetKernel(&e->kern.pair_first[d], e->lib, kJitPairFirst[d]);
         if (err == cudaSuccess) err = cudaLibraryGetKernel(&e->kern.pair[d], e->lib, kJitPair[d]);
-        if (err == cudaSuccess) err = cudaLibraryGetKernel(&e->kern.chain[d], e->lib, kJitChain[d]);
     }
     if (err != cudaSuccess) {
         (void)cudaGetLastError();

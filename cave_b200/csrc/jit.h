@@ -49,7 +49,6 @@ struct JitKernels {
     cudaKernel_t derived[2] = {nullptr, nullptr};
     cudaKernel_t pair_first[2] = {nullptr, nullptr};
     cudaKernel_t pair[2] = {nullptr, nullptr};
-    cudaKernel_t chain[2] = {nullptr, nullptr};  // pair[] running several passes in one cooperative launch
     explicit operator bool() const { return counting[0] != nullptr; }
     cudaKernel_t pick(bool first_tick, bool dense) const { return first_tick ? counting[dense] : derived[dense]; }
     cudaKernel_t pick2(bool first_pair, bool dense) const { return first_pair ? pair_first[dense] : pair[dense]; }
@@ -80,14 +79,6 @@ cudaError_t launch_stream_tick_jit(cudaKernel_t k, const StreamItem* items, uint
 cudaError_t launch_stream_tick2_jit(cudaKernel_t k, const StreamItem* items, uint32_t n_items, StripSim* sims,
                                     uint4* pool, uint32_t SX, uint32_t SXp, uint32_t threads, cudaStream_t st,
                                     bool pdl, int tick_arg, int src_sel);
-
-// `npasses` two-tick passes in one cooperative launch of a chain kernel (JitKernels::chain):
-// ticks tick_arg .. tick_arg + 2 npasses - 1, pass p reading copy src_sel ^ (p & 1). `flags`
-// holds one zeroed word per item (the items z-major, `ny` per z-row); see stream_tick2.cuh for the
-// plan's conditions. Fails (nothing launched) when the items cannot all be resident at once.
-cudaError_t launch_stream_tick2_chain_jit(cudaKernel_t k, const StreamItem* items, uint32_t n_items, StripSim* sims,
-                                          uint4* pool, uint32_t SX, uint32_t SXp, uint32_t threads, cudaStream_t st,
-                                          int tick_arg, int src_sel, uint32_t npasses, uint32_t* flags, uint32_t ny);
 
 // Dynamic shared memory of a two-tick launch with `rows` rows per CTA (incl. halo rows).
 size_t tick2_smem_bytes(uint32_t rows, uint32_t SX, uint32_t SXp);

@@ -285,43 +285,6 @@ cudaError_t launch_stream_tick2_jit(cudaKernel_t k, const StreamItem* items, uin
     return e;
 }
 
-cudaError_t launch_stream_tick2_chain_jit(cudaKernel_t k, const StreamItem* items, uint32_t n_items, StripSim* sims,
-                                          uint4* pool, uint32_t SX, uint32_t SXp, uint32_t threads, cudaStream_t st,
-                                          int tick_arg, int src_sel, uint32_t npasses, uint32_t* flags, uint32_t ny) {
-    uint32_t lg = 0;
-    while ((1u << lg) < SXp) lg++;
-    const size_t smem = stream2_smem_bytes(tick2_geometry().rows_per_thread * threads / SXp, SX, SXp);
-    {
-        static std::mutex mu;
-        static std::map<std::pair<const void*, int>, size_t> configured;
-        int dev = 0;
-        cudaError_t e = cudaGetDevice(&dev);
-        if (e != cudaSuccess) return e;
-        std::lock_guard<std::mutex> lock(mu);
-        size_t& c = configured[{(const void*)k, dev}];
-        if (smem > c) {
-            e = cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
-            c = smem;
-        }
-    }
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(n_items);
-    cfg.blockDim = dim3(threads);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;  // every CTA resident: they wait on one another
-    attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    void* args[] = {(void*)&items, (void*)&sims, (void*)&pool, (void*)&lg, (void*)&tick_arg, (void*)&src_sel,
-                    (void*)&npasses, (void*)&flags, (void*)&ny};
-    const cudaError_t e = cudaLaunchKernelExC(&cfg, (const void*)k, args);
-    if (e == cudaSuccess) jit_count_launch();
-    return e;
-}
-
 cudaError_t launch_stream_tick(int nb, int nt, const DeviceRule* param_rule, const StreamItem* items,
                                uint32_t n_items, StripSim* sims, uint4* pool, uint32_t SX, uint32_t SXp,
                                uint32_t threads, cudaStream_t st, bool pdl, int tick_arg) {

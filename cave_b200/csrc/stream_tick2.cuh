@@ -42,54 +42,10 @@ __host__ __device__ inline size_t stream2_smem_bytes(uint32_t rows, uint32_t SX,
 // kFirst: the run's first launch (ticks 0 and 1). kDense: the launch guarantees SX == SXp.
 // kStrips: rows per thread. src_sel: the cell copy (0 / 1) holding the input; the output goes to
 // the other one.
-// kChain: the launch runs `npasses` two-tick passes (ticks tick_arg + 2p, + 2p + 1, reading copy
-// src_sel ^ (p & 1)) instead of one. It must be a cooperative launch of one CTA per item, the
-// items laid out z-major with `chain_ny` items per z-row and every tile at least two rows high
-// and every slab at least two planes deep except the last ones: a pass reads the previous
-// pass's output in its tile and the two rows / planes around it, which only the eight
-// neighbouring items write. Before pass p > 0 a CTA waits until each neighbour's flag
-// (chain_flags[item], zeroed before the launch) reads p, i.e. the neighbour has written its part
-// of pass p - 1 and no longer reads the copy pass p overwrites; after each pass it publishes its
-// own. The waits are bounded: a CTA that gives up (or sees a neighbour that gave up) marks its
-// flag as aborted, raises kErrWaitTimeout and stops.
-constexpr uint32_t kChainAbort = 0xFFFFFFFFu;
-
-// Waits (one thread) until every neighbour of item i in the ny-wide item grid has published
-// `need`; 0 when they have, 1 after kWaitLimitNs, 2 when a neighbour aborted.
-__device__ __forceinline__ uint32_t chain_wait(const uint32_t* flags, uint32_t i, uint32_t ny, uint32_t n,
-                                               uint32_t need) {
-    const int iy = (int)(i % ny), iz = (int)(i / ny), nz = (int)(n / ny);
-    uint64_t t0 = 0;
-    for (bool first = true;; first = false) {
-        bool ready = true, aborted = false;
-#pragma unroll
-        for (int dz = -1; dz <= 1; dz++) {
-#pragma unroll
-            for (int dy = -1; dy <= 1; dy++) {
-                const int jy = iy + dy, jz = iz + dz;
-                if ((dy == 0 && dz == 0) || jy < 0 || jy >= (int)ny || jz < 0 || jz >= nz) continue;
-                const uint32_t v = ld_acquire_gpu(flags + (size_t)jz * ny + jy);
-                aborted |= v == kChainAbort;
-                ready &= v >= need;
-            }
-        }
-        if (aborted) return 2;
-        if (ready) return 0;
-        if (first) {
-            t0 = global_ns();
-        } else if (global_ns() - t0 > kWaitLimitNs) {
-            return 1;
-        }
-    }
-}
-
-template <int NB, class Fixed, bool kFirst, bool kDense, int kStrips, bool kChain = false>
+template <int NB, class Fixed, bool kFirst, bool kDense, int kStrips>
 __device__ __forceinline__ void stream_tick2_body(const StreamItem* __restrict__ items, StripSim* sims, uint4* pool,
-                                                  uint32_t sxp_log2, int tick_arg, int src_sel, uint32_t npasses = 1,
-                                                  uint32_t* chain_flags = nullptr, uint32_t chain_ny = 1) {
+                                                  uint32_t sxp_log2, int tick_arg, int src_sel) {
     static_assert(Fixed::kFixed, "the two-tick kernel is compiled for one rule");
-    static_assert(!(kChain && kFirst), "a chained launch follows the run's first pair");
-    __shared__ uint32_t s_abort;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ uint32_t red[32][21];
     const StreamItem it = items[blockIdx.x];
@@ -151,37 +107,9 @@ __device__ __forceinline__ void stream_tick2_body(const StreamItem* __restrict__
 #endif
     const size_t ring_off = (size_t)yy0 * SX + sx, x_off = (size_t)yy0 * SXp + sx;
 
-  for (uint32_t pass = 0; pass < npasses; pass++) {
-    const uint32_t tick = (uint32_t)tick_arg + 2u * pass;
-    const int sel = src_sel ^ (int)(pass & 1u);
-    const uint4* src = reinterpret_cast<const uint4*>(reinterpret_cast<unsigned char*>(pool) + (sel ? buf1 : buf0));
-    uint4* dst = reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(pool) + (sel ? buf0 : buf1));
-    if constexpr (kChain) {
-        if (pass > 0) {
-            // the neighbours' part of the previous pass; then fresh ring barriers (no copy is in
-            // flight: every fetch of the previous pass was waited for)
-            if (threadIdx.x == 0) {
-                const uint32_t w = chain_wait(chain_flags, blockIdx.x, chain_ny, gridDim.x, pass);
-                s_abort = w;
-                if (w == 0) {
-                    fence_proxy_async_all();  // the copies below read what the generic stores wrote
-                    for (int q = 0; q < kRing; q++) {
-                        mbar_inval(&bars[q]);
-                        mbar_init(&bars[q], 1);
-                    }
-                    mbar_init_fence();
-                }
-            }
-            __syncthreads();
-            if (s_abort) {
-                if (threadIdx.x == 0) {
-                    st_release_gpu(chain_flags + blockIdx.x, kChainAbort);
-                    atomicOr(&sim->error, kErrWaitTimeout);
-                }
-                break;
-            }
-        }
-    }
+    const uint32_t tick = (uint32_t)tick_arg;
+    const uint4* src = reinterpret_cast<const uint4*>(reinterpret_cast<unsigned char*>(pool) + (src_sel ? buf1 : buf0));
+    uint4* dst = reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(pool) + (src_sel ? buf0 : buf1));
 
     // Thread 0 fills ring slot f % kRing with input plane f; a plane outside the grid completes
     // its slot's phase with a plain arrive (every fetch advances its slot by one phase).
@@ -206,7 +134,7 @@ __device__ __forceinline__ void stream_tick2_body(const StreamItem* __restrict__
         for (int f = 0; f < kRing; f++) issue(f);
     }
     const uint4* my_ring = ring + (size_t)yy0 * SX + sx;  // row q at + q * SX
-    if (kDense && pass == 0) {
+    if constexpr (kDense) {
 #pragma unroll
         for (int q = 0; q < kStrips; q++) {
             if (!has[q]) {
@@ -524,13 +452,6 @@ __device__ __forceinline__ void stream_tick2_body(const StreamItem* __restrict__
     }
     }
     }
-    if constexpr (kChain) {
-        // publish this pass: every thread's stores visible GPU-wide, then the flag
-        __threadfence();
-        __syncthreads();
-        if (threadIdx.x == 0) st_release_gpu(chain_flags + blockIdx.x, pass + 1u);
-    }
-  }  // passes
 }
 
 }  // namespace cave

@@ -1,10 +1,9 @@
 """GPU parity of the rule-specialised tick kernels (NVRTC): with CAVE_JIT=sync every cave_run and
 cave_render_step below runs the kernels compiled for its rule, checked bit-exact against the
 oracle (every cell, every per-tick statistic, GridInfo), and the launch counter proves that the
-specialised kernels, not the generic one, did the ticks. Every cave_run case runs three ways: two
-ticks per launch with the pairs after the first chained into one cooperative launch where the tiling
-allows it (the default; an odd tick count starts with one single-tick launch), two ticks per launch
-with one launch per pair (CAVE_TICK2_CHAIN=0), and one tick per launch (CAVE_TICK2=0)."""
+specialised kernels, not the generic one, did the ticks. Every cave_run case runs twice: with
+two ticks per launch (the default; an odd tick count starts with one single-tick launch) and with
+CAVE_TICK2=0 (one tick per launch)."""
 import os
 
 import numpy as np
@@ -16,22 +15,14 @@ import oracle as O
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(params=["chain", "pairs", "single"], autouse=True)
+@pytest.fixture(params=["pairs", "single"], autouse=True)
 def tick2(request, monkeypatch):
-    monkeypatch.setenv("CAVE_TICK2", "0" if request.param == "single" else "1")
-    monkeypatch.setenv("CAVE_TICK2_CHAIN", "1" if request.param == "chain" else "0")
-    return request.param
+    monkeypatch.setenv("CAVE_TICK2", "1" if request.param == "pairs" else "0")
+    return request.param == "pairs"
 
 
-def expected_launches(nticks, mode):
-    """Launch counts a run may take: the chain needs a tiling whose tiles are two rows high and
-    slabs two planes deep, else its pairs launch one by one."""
-    if mode == "single" or nticks < 2:
-        return {nticks}
-    pairs = (nticks & 1) + nticks // 2
-    if mode == "pairs" or nticks // 2 < 3:
-        return {pairs}
-    return {pairs, (nticks & 1) + 2}
+def expected_launches(nticks, pairs):
+    return (nticks & 1) + nticks // 2 if pairs and nticks >= 2 else nticks
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -56,7 +47,7 @@ def random_states(rng, X, Y, Z, maxcs, p_alive=0.35, p_other=0.15):
     return O.pack(s)
 
 
-def run_and_check(ctx, X, Y, Z, params_np, init, nticks, max_ticks=10 ** 6, chains=False):
+def run_and_check(ctx, X, Y, Z, params_np, init, nticks, max_ticks=10 ** 6):
     p = cb.SimParams(*[int(v) for v in params_np])
     cells, expect = init, []
     for _ in range(nticks):
@@ -68,11 +59,8 @@ def run_and_check(ctx, X, Y, Z, params_np, init, nticks, max_ticks=10 ** 6, chai
         sts, info = g.run(p, nticks, max_ticks)
         got_cells = g.download()
     _, launches1 = cb.jit_stats()
-    mode = "single" if os.environ.get("CAVE_TICK2") == "0" else "chain" if os.environ.get("CAVE_TICK2_CHAIN") == "1" \
-        else "pairs"
-    assert launches1 - launches0 in expected_launches(nticks, mode), "the ticks did not run on the specialised kernels"
-    if chains and mode == "chain":  # a tiling the chain runs on: one launch for the pairs after the first
-        assert launches1 - launches0 == (nticks & 1) + 2, "the pairs were not chained"
+    pairs = os.environ.get("CAVE_TICK2") != "0"
+    assert launches1 - launches0 == expected_launches(nticks, pairs), "the ticks did not run on the specialised kernels"
     assert np.array_equal(got_cells, cells), "cells differ"
     for t in range(nticks):
         assert sts[t].as_tuple() == expect[t], f"statistics differ at tick {t + 1}"
@@ -138,15 +126,13 @@ def test_pair_tilings(ctx, dims):
 
 @pytest.mark.parametrize("dims,nticks", [((512, 200, 33), 9), ((512, 90, 150), 10), ((480, 150, 300), 8),
                                          ((64, 40, 1200), 12), ((256, 256, 256), 7)])
-def test_chain_tilings(ctx, dims, nticks):
-    """Tilings the chained passes run on -- a last slab of one plane, partial strips (480 cells per
-    row), one y-tile with 600 small CTAs, many y-tiles -- Moore neighbourhood, several passes:
-    every pass equals the oracle's ticks, and in the default mode the pairs after the first ran as
-    one chained launch."""
+def test_long_slab_tilings(ctx, dims, nticks):
+    """Slabs of two planes or more with a last slab of one plane, partial strips (480 cells per
+    row), one y-tile with 600 small CTAs, many y-tiles; Moore neighbourhood, several launches:
+    every tick equals the oracle's."""
     X, Y, Z = dims
     rng = np.random.default_rng(X + 5 * Y + 11 * Z)
-    run_and_check(ctx, X, Y, Z, O.make_params(15, 0x7, 0x10, 0x18), random_states(rng, X, Y, Z, 15), nticks,
-                  chains=True)
+    run_and_check(ctx, X, Y, Z, O.make_params(15, 0x7, 0x10, 0x18), random_states(rng, X, Y, Z, 15), nticks)
 
 
 def test_prepare_then_async(ctx):
