@@ -203,14 +203,15 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
     TickAcc acc;
     acc.reset(SX != 0u ? 1u : 0u);  // SX >= 1: a 1 the compiler cannot fold
     uint32_t xbits[kStrips];
-    uint4* my_dst[kStrips];
+    // strip index of each row in a plane of the output copy (a copy holds at most 2^25 strips)
+    uint32_t dst_row[kStrips];
 #pragma unroll
     for (int q = 0; q < kStrips; q++) {
         xbits[q] = 0u;
-        my_dst[q] = dst + ((size_t)max(y[q], 0) * SX + sx);
+        dst_row[q] = (uint32_t)max(y[q], 0) * SX + sx;
     }
     uint4* my_x = xch + (size_t)yy0 * SXp + sx;  // row q at + q * SXp
-    const size_t plane_stride = (size_t)Y * SX;
+    const uint32_t plane_strips = Y * SX;
 
     int zo = zfirst + zstep;
     // Fetch f is the (f / kRing)-th use of slot f % kRing, so the phase parity to wait for is
@@ -274,6 +275,7 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
             fence_proxy_async();
             issue(f + kRing);
         }
+        uint32_t zany = 0u;  // the counted cells' non-zero masks of this plane (its z-extent)
 #pragma unroll
         for (int q = 0; q < kStrips; q++) {
             if (outp[q]) {
@@ -295,11 +297,15 @@ __device__ __forceinline__ void stream_tick_body(const StreamItem* __restrict__ 
                 }
                 uint32_t cnt[count_bits(NB)];
                 P::combine(pc[q], psm, psp, cnt);
-                const uint4 n = update_strip<NB, NT, kCountZero, Fixed::kFullRange, kPop>(
-                    s_c[q], r_c[q].a, cnt, valid, R, acc, xbits[q], (uint32_t)zo);
-                if (CAVE_IN_BOUNDS((size_t)max(y[q], 0) * SX + sx + (size_t)zo * plane_stride, copy_n, err))
-                    my_dst[q][(size_t)zo * plane_stride] = n;
+                const uint4 n = update_strip<NB, NT, kCountZero, Fixed::kFullRange, kPop, false>(
+                    s_c[q], r_c[q].a, cnt, valid, R, acc, xbits[q], (uint32_t)zo, true, &zany);
+                const uint32_t di = (uint32_t)zo * plane_strips + dst_row[q];
+                if (CAVE_IN_BOUNDS(di, copy_n, err)) dst[di] = n;
             }
+        }
+        if (zany) {
+            acc.zmin = min(acc.zmin, (uint32_t)zo);
+            acc.zmax = max(acc.zmax, (uint32_t)zo);
         }
 #pragma unroll
         for (int q = 0; q < kStrips; q++) {
