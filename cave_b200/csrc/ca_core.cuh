@@ -62,28 +62,27 @@ __device__ __forceinline__ void add3(const uint32_t* a, const uint32_t* b, const
 }
 
 // ---------------------------------------------------------------- rules
-// LUT evaluation by a mux tree over the count planes; leaves are the table bits.
-template <int NBITS>
-__device__ __forceinline__ uint32_t lut_tree(const uint32_t* c, uint32_t lut) {
-    constexpr int NL = 1 << NBITS;
-    uint32_t v[NL / 2];
-#pragma unroll
-    for (int j = 0; j < NL / 2; j++) {
-        const uint32_t t0 = 0u - ((lut >> (2 * j)) & 1u);
-        const uint32_t t1 = 0u - ((lut >> (2 * j + 1)) & 1u);
-        v[j] = (c[0] & t1) | (~c[0] & t0);
+// Table bit `lut[k]` at count k = (c[0..BIT]) + LO, for counts up to MAXC: a mux tree over the
+// count planes whose branches above MAXC are left out -- a count there never occurs, so a
+// subtree whose upper half lies wholly above MAXC is its lower half alone: MAXC logic operations
+// per table (lut_tree_ops) instead of 2^bits - 1, e.g. FE 19 instead of 31, C 8 instead of 15.
+template <int BIT, int LO, int MAXC>
+__device__ __forceinline__ uint32_t lut_tree_bounded(const uint32_t* c, uint32_t lut) {
+    if constexpr (BIT < 0) {
+        return 0u - ((lut >> LO) & 1u);
+    } else if constexpr (LO + (1 << BIT) > MAXC) {
+        return lut_tree_bounded<BIT - 1, LO, MAXC>(c, lut);
+    } else {
+        const uint32_t hi = lut_tree_bounded<BIT - 1, LO + (1 << BIT), MAXC>(c, lut);
+        const uint32_t lo = lut_tree_bounded<BIT - 1, LO, MAXC>(c, lut);
+        return (c[BIT] & hi) | (~c[BIT] & lo);
     }
-#pragma unroll
-    for (int lvl = 1; lvl < NBITS; lvl++) {
-#pragma unroll
-        for (int j = 0; j < (NL >> (lvl + 1)); j++) v[j] = (c[lvl] & v[2 * j + 1]) | (~c[lvl] & v[2 * j]);
-    }
-    return v[0];
 }
 
 // (survive-hit, birth-hit) planes for count planes c. NT = number of sparse terms the rule
-// was built with (1..kMaxTerms), or 0 for the mux-tree evaluation of the two tables.
-template <int NBITS, int NT>
+// was built with (1..kMaxTerms), or 0 for the mux-tree evaluation of the two tables; MAXC = the
+// largest count the planes can hold (the tree leaves out the branches above it).
+template <int NBITS, int NT, int MAXC = (1 << NBITS) - 1>
 __device__ __forceinline__ void eval_rule(const uint32_t* c, const DeviceRule& r, uint32_t& hs, uint32_t& hb) {
     if constexpr (NT > 0) {
         uint32_t as = 0u, ab = 0u;
@@ -99,8 +98,8 @@ __device__ __forceinline__ void eval_rule(const uint32_t* c, const DeviceRule& r
         hs = as;
         hb = ab;
     } else {
-        hs = lut_tree<NBITS>(c, r.lut_s);
-        hb = lut_tree<NBITS>(c, r.lut_b);
+        hs = lut_tree_bounded<NBITS - 1, 0, MAXC>(c, r.lut_s);
+        hb = lut_tree_bounded<NBITS - 1, 0, MAXC>(c, r.lut_b);
     }
 }
 
@@ -291,7 +290,7 @@ __device__ __forceinline__ uint4 update_strip(uint4 s, uint32_t a, const uint32_
                                               const DeviceRule& r, TickAcc& acc, uint32_t& xbits, uint32_t z,
                                               bool count = true, uint32_t* zany = nullptr) {
     uint32_t hs, hb;
-    eval_rule<count_bits(NB), NT>(cnt, r, hs, hb);
+    eval_rule<count_bits(NB), NT, max_count(NB)>(cnt, r, hs, hb);
     const uint32_t nz = s.x | s.y | s.z | s.w;
     const uint32_t zero = ~nz & valid;
     const uint32_t sv = a & hs;

@@ -73,6 +73,14 @@ CAVE_HD constexpr int max_count(int nb) {
     return nb == 0 ? 0 : nb == 1 ? 7 : nb == 2 ? 12 : nb == 3 ? 19 : nb == 4 ? 8 : nb == 5 ? 15 : nb == 6 ? 20 : 27;
 }
 
+// Logic operations of the rule table's mux tree for counts up to maxc (ca_core.cuh,
+// lut_tree_bounded<bit, lo, maxc>): one per leaf above the first, i.e. maxc for lo = 0.
+CAVE_HD constexpr int lut_tree_ops(int bit, int lo, int maxc) {
+    return bit < 0 ? 0
+           : lo + (1 << bit) > maxc ? lut_tree_ops(bit - 1, lo, maxc)
+                                    : lut_tree_ops(bit - 1, lo + (1 << bit), maxc) + lut_tree_ops(bit - 1, lo, maxc) + 1;
+}
+
 // Valid-cell mask of strip sx in a row of X cells.
 CAVE_HD inline uint32_t strip_valid(uint32_t sx, uint32_t X) {
     const uint32_t x0 = sx * 32u;

@@ -42,12 +42,12 @@ DeviceRule make_device_rule(const DecodedRule& d) {
     const uint64_t lb = (d.birth << 1) & keep;
     r.lut_s = (uint32_t)ls;
     r.lut_b = (uint32_t)lb;
-    // Sparse evaluation costs ~9 logic ops per distinct count value; the mux tree costs
-    // 2 * (2^bits - 1). Use whichever is cheaper.
+    // Sparse evaluation costs ~9 logic ops per distinct count value; the mux tree costs one op
+    // per table and reachable count (lut_tree_ops). Use whichever is cheaper.
     const uint32_t u = r.lut_s | r.lut_b;
     const int nterms = std::popcount(u);
     const int nbits = count_bits(nb);
-    const int tree_cost = 2 * ((1 << nbits) - 1);
+    const int tree_cost = 2 * lut_tree_ops(nbits - 1, 0, maxc);
     if (nterms <= kMaxSparseTerms && nterms * 9 < tree_cost) {
         int t = 0;
         for (int k = 0; k < 32; k++) {
