@@ -24,6 +24,7 @@
 #include "kernels.h"
 #include "engine.h"
 #include "rules.h"
+#include "trace.h"
 
 namespace cave {
 
@@ -218,6 +219,7 @@ cave_status cave_batch_add_sims(cave_batch* b, const cave_sim_desc* sims, uint64
 
 cave_status cave_batch_launch(cave_batch* b) {
     if (!b) return CAVE_ERR_INVALID_ARG;
+    TraceRange trace("cave_batch_launch");
     cave_ctx* ctx = b->ctx;
     if (b->launched) return set_error(ctx, CAVE_ERR_INVALID_ARG, "batch already launched");
     CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -469,6 +471,7 @@ cave_status cave_batch_poll(cave_batch* b) {
 
 cave_status cave_batch_results(cave_batch* b, cave_sim_result* out, uint64_t n) {
     if (!b || !b->launched || (n && !out) || n > b->launched_n) return CAVE_ERR_INVALID_ARG;
+    TraceRange trace("cave_batch_results");
     cave_ctx* ctx = b->ctx;
     CAVE_CUDA(ctx, cudaSetDevice(ctx->device));
     if (b->worker.joinable()) b->worker.join();
@@ -510,6 +513,7 @@ cave_status cave_batch_results(cave_batch* b, cave_sim_result* out, uint64_t n) 
 
 cave_status cave_batch_run_plain(cave_batch* b, uint32_t nslots, double* deviceSeconds) {
     if (!b || nslots == 0) return CAVE_ERR_INVALID_ARG;
+    TraceRange trace("cave_batch_run_plain");
     cave_ctx* ctx = b->ctx;
     if (b->launched) return set_error(ctx, CAVE_ERR_INVALID_ARG, "batch already launched");
     CAVE_CUDA(ctx, cudaSetDevice(ctx->device));

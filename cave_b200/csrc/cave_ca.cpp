@@ -14,6 +14,7 @@
 #include "jit.h"
 #include "kernels.h"
 #include "rules.h"
+#include "trace.h"
 
 namespace cave {
 
@@ -307,6 +308,7 @@ struct DevTable {
 cave_status cave_step(cave_grid* g, const cave_sim_params* params, const uint64_t* validBitmasks, uint32_t nValid,
                       uint32_t maxRuleBits, uint32_t nticks, cave_tick_stats* per_tick) {
     if (!g || !params) return CAVE_ERR_INVALID_ARG;
+    TraceRange trace("cave_step");
     cave_ctx* ctx = g->ctx;
     DecodedRule d;
     if (!decode_params(*params, validBitmasks, nValid, maxRuleBits, d))
@@ -553,6 +555,7 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
                             const uint64_t* validBitmasks, uint32_t nValid, uint32_t maxRuleBits, uint32_t nticks,
                             uint32_t maxTicks, cave_tick_stats* per_tick, cave_grid_info* info) {
     if (!g || !params) return CAVE_ERR_INVALID_ARG;
+    TraceRange trace(host_in ? "cave_run_host" : "cave_run");
     cave_ctx* ctx = g->ctx;
     DecodedRule d;
     if (!decode_params(*params, validBitmasks, nValid, maxRuleBits, d))
@@ -701,6 +704,7 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
     cudaGraphExec_t gexec = nullptr;
     if (use_graph && e == cudaSuccess) e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed);
     uint32_t sel = 0, launches = 0;
+    nvtxRangePushA("ticks");
     if (kind == kRunJitPair) {
         uint32_t t = 0;
         if (lead && e == cudaSuccess) {
@@ -727,6 +731,7 @@ static cave_status run_impl(cave_grid* g, const uint32_t* host_in, uint32_t* hos
         record(ctx, 2);
         if (e == cudaSuccess) e = cudaGraphLaunch(gexec, ctx->stream);
     }
+    nvtxRangePop();
     if (e == cudaSuccess && nticks && jk)  // the last tick's population comes from the final grid
         e = launch_strip_stats(g->strips + (uint64_t)sel * nstrips, g->Y, g->Z, plan.SX, dtt + (nticks - 1),
                                (uint32_t)ctx->sm_count, ctx->stream);

@@ -1,5 +1,6 @@
 // engine.cpp -- see engine.h.
 #include "engine.h"
+#include "trace.h"
 
 #include <algorithm>
 #include <chrono>
@@ -980,6 +981,7 @@ cave_status Engine::finish_timing() {
 }
 
 cave_status Engine::step(bool* idle) {
+    TraceRange trace("engine_round");
     *idle = false;
     if (!ready_) return CAVE_ERR_INVALID_ARG;
     CAVE_CUDA(ctx_, cudaSetDevice(ctx_->device));

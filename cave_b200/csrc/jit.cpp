@@ -8,6 +8,7 @@
 // $XDG_CACHE_HOME/cave_b200 or ~/.cache/cave_b200; "off" disables the disk cache), named by a
 // hash of the sources, the options and the CUDA toolkit version the library was built with.
 #include "jit.h"
+#include "trace.h"
 
 #include <dlfcn.h>
 #include <nvrtc.h>
@@ -191,6 +192,7 @@ std::vector<std::string> options_for(const JitKey& k) {
 
 // Compiles the kernel for k (or reads it from the disk cache). No device is touched.
 bool compile_cubin(const JitKey& k, std::vector<char>* out, std::string* log) {
+    TraceRange trace("jit_compile");
     const std::vector<std::string> opts = options_for(k);
     uint64_t h = fnv1a(kJitUnit, std::strlen(kJitUnit));
     for (int i = 0; i < kJitSourceCount; i++) {

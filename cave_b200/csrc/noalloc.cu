@@ -19,6 +19,7 @@
 #include "context.h"
 #include "kernels.h"
 #include "rules.h"
+#include "trace.h"
 
 namespace cave {
 namespace {
@@ -90,6 +91,7 @@ extern "C" cave_status cave_run_noalloc(cave_ctx* ctx, const uint32_t* d_in, uin
                                         uint32_t nticks, uint32_t maxTicks, cave_tick_stats* d_per_tick,
                                         cave_grid_info* info) {
     if (!ctx || !params || !d_in || !d_out) return CAVE_ERR_INVALID_ARG;
+    TraceRange trace("cave_run_noalloc");
     DecodedRule d;
     if (!decode_params(*params, validBitmasks, nValid, maxRuleBits, d))
         return set_error(ctx, CAVE_ERR_INVALID_ARG, "rule index outside the valid-bitmask table");

@@ -15,6 +15,7 @@
 #include "jit.h"
 #include "kernels.h"
 #include "rules.h"
+#include "trace.h"
 
 using namespace cave;
 
@@ -31,6 +32,7 @@ uint64_t cave_render_skip_elements(uint32_t X, uint32_t Y, uint32_t Z) {
 cave_status cave_render_step(cave_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t X, uint32_t Y, uint32_t Z,
                              const cave_sim_params* params, uint32_t nticks, uint32_t* d_skip) {
     if (!ctx || !params || !d_in || !d_out) return CAVE_ERR_INVALID_ARG;
+    TraceRange trace("cave_render_step");
     if (X == 0 || Y == 0 || Z == 0 || (uint64_t)X * Y * Z >= (1ull << 32))
         return set_error(ctx, CAVE_ERR_INVALID_ARG, "grid volume must be in [1, 2^32)");
     DecodedRule d;

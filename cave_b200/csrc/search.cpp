@@ -24,6 +24,7 @@
 #include "context.h"
 #include "kernels.h"
 #include "rules.h"
+#include "trace.h"
 
 namespace cave {
 
@@ -293,6 +294,7 @@ static cave_status run_batched(cave_ctx* ctx, const cave_search_config& c, const
             break;
         }
         // ---- one wave
+        TraceRange trace("search_wave");
         cave_batch* b = nullptr;
         cave_status rc = cave_batch_create(ctx, &b);
         if (rc) return rc;
