@@ -81,18 +81,18 @@ class SearchConfig(ctypes.Structure):
                 ("densitySweepMax", ctypes.c_float), ("densitySweepStep", ctypes.c_float), ("seedRuns", u32),
                 ("faces", u32), ("edges", u32), ("corners", u32), ("wrap", u32), ("minMaxCellState", u32),
                 ("maxMaxCellState", u32), ("maxTicks", u32), ("maxRuleBits", u32), ("chunksPerConfig", u32),
-                ("outputFolder", ctypes.c_char_p)]
+                ("outputFolder", ctypes.c_char_p), ("resume", u32), ("pad", u32)]
 
 
 class SearchSummary(ctypes.Structure):
     _fields_ = [("sims", u64), ("viable", u64), ("possible", u64), ("unviable", u64), ("ticks", u64),
                 ("cellUpdates", u64), ("chunks", u32), ("uniqueRules", u32), ("deviceSeconds", ctypes.c_double),
-                ("wallSeconds", ctypes.c_double), ("stopped", u32), ("pad", u32)]
+                ("wallSeconds", ctypes.c_double), ("stopped", u32), ("pad", u32), ("resumedSims", u64)]
 
 
 def search_config(grid=49, spawn=11, spawn_mode="filled", density=0.5, neighborhood="F", min_cs=3, max_cs=10,
                   ticks=50, max_rule_bits=0, chunks_per_config=1, seed_runs=1, grid_sweep=None, density_sweep=None,
-                  output=None) -> SearchConfig:
+                  output=None, resume=False) -> SearchConfig:
     """SearchConfig from the reference CLI's search flags (defaults as src/main.cpp:29-44, except
     --chunks-per-config, whose partitions only change scheduling)."""
     c = SearchConfig()
@@ -111,6 +111,7 @@ def search_config(grid=49, spawn=11, spawn_mode="filled", density=0.5, neighborh
     c.maxRuleBits = max_rule_bits
     c.chunksPerConfig = chunks_per_config
     c.outputFolder = (output.encode() if output else None)
+    c.resume = 1 if resume else 0
     return c
 
 

@@ -247,6 +247,50 @@ struct ChunkWriter {
     }
 };
 
+// Simulations of chunk ci: every (slot, survival, birth) of the chunk's survival range.
+static uint64_t chunk_sim_count(const Sweep& s, size_t ci) {
+    uint64_t n = 0;
+    for (const GridConfig& g : s.configs) {
+        uint64_t lo, hi;
+        survival_range(g, s.chunks[ci], lo, hi);
+        if (hi >= lo) n += (hi - lo + 1) * g.maxPermutation;
+    }
+    return n;
+}
+
+// Reads a chunk's three JSONL files back (resume). True when they hold exactly the chunk's
+// `expected` results, every line exactly as result_line writes it; `outs` then holds them.
+static bool read_chunk(const std::string& prefix, uint64_t expected, std::vector<Outcome>& outs) {
+    const char* names[3] = {"_viable.jsonl", "_possible.jsonl", "_unviable.jsonl"};
+    outs.clear();
+    for (uint32_t k = 0; k < 3; k++) {
+        std::ifstream f(prefix + names[k]);
+        if (!f.is_open()) return false;
+        std::string line;
+        while (std::getline(f, line)) {
+            unsigned long long birth = 0, shape = 0, surv = 0;
+            unsigned fin = 0, mx = 0, ticks = 0, births = 0, deaths = 0;
+            if (std::sscanf(line.c_str(),
+                            "{\"birthAndMaxCellStateRules\":%llu,\"finalAliveCount\":%u,\"maxAliveCount\":%u,"
+                            "\"shapeAndGridConfiguration\":%llu,\"survivalAndNeighborhoodRules\":%llu,"
+                            "\"ticksSurvived\":%u,\"totalBirths\":%u,\"totalDeaths\":%u}",
+                            &birth, &fin, &mx, &shape, &surv, &ticks, &births, &deaths) != 8)
+                return false;
+            Outcome o{};
+            o.params = cave_sim_params{birth, surv, shape};
+            o.info.finalAliveCount = fin;
+            o.info.maxAliveCount = mx;
+            o.info.numberOfSimulationTicksSurvived = ticks;
+            o.info.totalNumberOfCellsThatWereBorn = births;
+            o.info.totalNumberOfCellsThatDied = deaths;
+            o.category = k;
+            if (result_line(o) != line || outs.size() >= expected) return false;
+            outs.push_back(o);
+        }
+    }
+    return outs.size() == expected;
+}
+
 // Results of one chunk as they arrive (the chunk's index and its outcomes in rule order).
 using ResultSink = std::function<cave_status(size_t chunk, const std::vector<Outcome>& outs)>;
 
@@ -265,7 +309,8 @@ static bool stop_requested(cave_ctx* ctx) { return ctx->search_stop.load(std::me
 // walks them), run in waves of up to wave_sims() simulations: one batch per wave, holding the
 // initial grids and K-index tables of the chunks the wave touches.
 static cave_status run_batched(cave_ctx* ctx, const cave_search_config& c, const Sweep& s, const ResultSink& sink,
-                               uint64_t limit, double& dev_s, uint64_t& nsims, bool& stopped) {
+                               const std::vector<char>& skip, uint64_t limit, double& dev_s, uint64_t& nsims,
+                               bool& stopped) {
     struct Piece {
         uint32_t chunk, gi;
         uint64_t sv, bi;  // first simulation of the piece
@@ -312,6 +357,10 @@ static cave_status run_batched(cave_ctx* ctx, const cave_search_config& c, const
         std::vector<cave_sim_desc> descs;
         std::vector<uint32_t> owner;  // chunk of each simulation
         while (ci < s.chunks.size() && descs.size() < per_wave && !(limit && nsims + descs.size() >= limit)) {
+            if (!loaded && skip[ci]) {  // its results were read back from its files
+                ci++;
+                continue;
+            }
             if (!loaded) {
                 sims_of.clear();
                 chunk_sims(ci, sims_of);
@@ -378,7 +427,8 @@ static cave_status run_batched(cave_ctx* ctx, const cave_search_config& c, const
 // initial cells, launch the step (with the fused manager) once per slot, fence, read the copy
 // buffers and record finished rules.
 static cave_status run_plain(cave_ctx* ctx, const cave_search_config& c, const Sweep& s, const ResultSink& sink,
-                             uint64_t limit, double& dev_s, uint64_t& nsims, bool& stopped) {
+                             const std::vector<char>& skip, uint64_t limit, double& dev_s, uint64_t& nsims,
+                             bool& stopped) {
     nsims = 0;
     stopped = false;
     double dev_ms = 0;
@@ -390,6 +440,7 @@ static cave_status run_plain(cave_ctx* ctx, const cave_search_config& c, const S
             stopped = true;
             break;
         }
+        if (skip[ci]) continue;  // its results were read back from its files
         const Chunk& ch = s.chunks[ci];
         const uint32_t nslot = (uint32_t)s.configs.size();
         std::vector<Outcome> outs;  // this chunk's results, handed over when it completes
@@ -559,11 +610,30 @@ cave_status cave_search_run(cave_ctx* ctx, const cave_search_config* config, uin
         chunk_done[ci] = 1;
         return writer.write(ctx, ci, outs);
     };
+    // resume: chunks whose files already hold all their results are read back, not run
+    std::vector<char> skip(s.chunks.size(), 0);
+    if (c.resume && !s.folder.empty()) {
+        std::vector<Outcome> outs;
+        for (size_t ci = 0; ci < s.chunks.size(); ci++) {
+            if (!read_chunk(s.folder + chunk_prefix(s, s.chunks[ci]), chunk_sim_count(s, ci), outs)) continue;
+            skip[ci] = 1;
+            const Chunk& ch = s.chunks[ci];
+            for (const Outcome& o : outs) {
+                sum.sims++;
+                sum.resumedSims++;
+                (o.category == 0 ? sum.viable : o.category == 1 ? sum.possible : sum.unviable)++;
+                sum.ticks += o.info.numberOfSimulationTicksSurvived;
+                sum.cellUpdates += (uint64_t)o.info.numberOfSimulationTicksSurvived * ch.X * ch.Y * ch.Z;
+                aggregate(agg, o);
+            }
+            chunk_done[ci] = 1;
+        }
+    }
     double dev_s = 0;
     uint64_t nsims = 0;
     bool stopped = false;
-    cave_status rc = mode == 0 ? run_batched(ctx, c, s, sink, simLimit, dev_s, nsims, stopped)
-                               : run_plain(ctx, c, s, sink, simLimit, dev_s, nsims, stopped);
+    cave_status rc = mode == 0 ? run_batched(ctx, c, s, sink, skip, simLimit, dev_s, nsims, stopped)
+                               : run_plain(ctx, c, s, sink, skip, simLimit, dev_s, nsims, stopped);
     if (rc) return rc;
     if (!s.folder.empty()) {
         if (!stopped) {

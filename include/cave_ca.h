@@ -441,6 +441,12 @@ typedef struct {
     uint32_t maxRuleBits;                         /* --max-rule-bits                      */
     uint32_t chunksPerConfig;                     /* --chunks-per-config                  */
     const char* outputFolder;                     /* --output (NULL or "" = no files)     */
+    uint32_t resume;   /* 1: a chunk whose three JSONL files already hold all its results (a
+                          sweep run before into the same folder, stopped or cut short) is not
+                          run again: its lines go into the aggregate and the summary as read;
+                          incomplete chunks are rewritten (the reference resumes at script
+                          level, bench_grand_resume.ps1)                                   */
+    uint32_t pad;
 } cave_search_config;
 
 typedef struct {
@@ -454,6 +460,8 @@ typedef struct {
     double wallSeconds;      /* whole call                                            */
     uint32_t stopped;        /* 1: cave_search_stop ended the sweep early             */
     uint32_t pad;
+    uint64_t resumedSims;    /* of sims: read from complete chunk files (resume), not run;
+                                the other totals cover them too                         */
 } cave_search_summary;
 
 /* Runs a whole sweep as SearchMode::OnFrame does (searchMode.cpp:49-218 expansion,

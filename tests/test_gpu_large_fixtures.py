@@ -2,7 +2,7 @@
 
 The benchmark workload: 256^3 and 512^3 cubes, Moore neighbourhood, maxCellState 15, survival
 {4,5}, birth {5}, 40% fill by the reference's cell hash with seed 0, stepped 100 and 1000 ticks
-by cave_run with statistics every tick. That rule settles into a still life within about 100
+by cave_run with statistics every tick (1024^3: 20 and 200 ticks, out of L2). That rule settles into a still life within about 100
 ticks, so "active" entries keep every tick busy at the same geometries (Moore C=4 B{5,6,7}
 S{5,6,7,8} at 256^3 and 512^3, FE C=6 B{4,5} S{3,4,5,6} at 256^3). Each runs on the
 rule-specialised tick kernels (CAVE_JIT=sync; runs of 100 or more ticks also take the tile-timing
@@ -23,7 +23,7 @@ import cave_b200 as cb
 pytestmark = pytest.mark.gpu
 
 FIXTURE = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "large_fixtures.json")))
-CASES = [(name, int(T)) for name in ("256", "512", "active256", "active512", "activeFE256") if name in FIXTURE
+CASES = [(name, int(T)) for name in ("256", "512", "1024", "active256", "active512", "activeFE256") if name in FIXTURE
          for T in FIXTURE[name]["checkpoints"]]
 
 

@@ -246,3 +246,29 @@ def test_unwritable_output_folder_is_an_io_error(ctx, tmp_path):
     with pytest.raises(cb.CaveError) as e:
         cb.search_run(ctx, cfg)
     assert e.value.code == cb.ERR_IO
+
+
+@pytest.mark.parametrize("plain", [False, True])
+def test_resume_reads_complete_chunks_and_reruns_the_rest(ctx, tmp_path, monkeypatch, plain):
+    """resume: a sweep cut short (a simulation limit in the middle of a chunk) left complete,
+    partial and missing chunk files; run again into the same folder with resume, it reads the
+    complete chunks back instead of running them, rewrites the partial one, runs the missing
+    ones, and every file -- the aggregate included -- equals a fresh run's."""
+    monkeypatch.setenv("CAVE_SEARCH_WAVE_SIMS", "512")
+    G, T = 7, 6
+    kw = dict(grid=G, spawn=5, spawn_mode="random", neighborhood="F", min_cs=2, max_cs=3, ticks=T, seed_runs=3)
+    fresh, part = str(tmp_path / "fresh") + "/", str(tmp_path / "part") + "/"
+    full = cb.search_run(ctx, cb.search_config(output=fresh, **kw), plain=plain)
+    per_chunk = full.sims // full.chunks
+    cut = cb.search_run(ctx, cb.search_config(output=part, **kw), plain=plain, sim_limit=per_chunk + per_chunk // 2)
+    assert per_chunk < cut.sims < full.sims
+    again = cb.search_run(ctx, cb.search_config(output=part, resume=True, **kw), plain=plain)
+    assert again.resumedSims >= per_chunk and again.resumedSims % per_chunk == 0
+    assert again.resumedSims < full.sims
+    for k in ("sims", "viable", "possible", "unviable", "ticks", "uniqueRules"):
+        assert getattr(again, k) == getattr(full, k), k
+    names = sorted(os.path.relpath(p, fresh) for p in glob.glob(os.path.join(fresh, "**", "*.jsonl"), recursive=True))
+    assert names == sorted(os.path.relpath(p, part) for p in glob.glob(os.path.join(part, "**", "*.jsonl"),
+                                                                       recursive=True))
+    for n in names:
+        assert open(os.path.join(part, n)).read() == open(os.path.join(fresh, n)).read(), n
