@@ -144,6 +144,11 @@ class ServerOptions(ctypes.Structure):
                 ("tiledOnly", u32), ("maxActiveCells", u64), ("requestDeadlineSeconds", ctypes.c_double)]
 
 
+class RequestProgress(ctypes.Structure):
+    _fields_ = [("total", u64), ("done", u64), ("viable", u64), ("possible", u64), ("unviable", u64),
+                ("complete", u32), ("expired", u32)]
+
+
 class ServerStats(ctypes.Structure):
     _fields_ = [("submitted", u64), ("completed", u64), ("simsCompleted", u64), ("cellUpdates", u64),
                 ("p50LatencySeconds", ctypes.c_double), ("p99LatencySeconds", ctypes.c_double),
@@ -218,6 +223,7 @@ _SIGS = {
     "cave_server_poll": (i32, [ctypes.c_void_p, P(u64), u64, P(u64)]),
     "cave_server_wait": (i32, [ctypes.c_void_p, u64, ctypes.c_double]),
     "cave_server_cancel": (i32, [ctypes.c_void_p, u64]),
+    "cave_server_progress": (i32, [ctypes.c_void_p, u64, ctypes.c_void_p]),
     "cave_server_fetch": (i32, [ctypes.c_void_p, u64, ctypes.c_void_p, u64, P(ctypes.c_double)]),
     "cave_server_get_stats": (i32, [ctypes.c_void_p, P(ServerStats)]),
     "cave_render_buffer_elements": (u64, [u32, u32, u32]),
@@ -638,6 +644,12 @@ class Server:
             return False
         self.ctx.check(rc, "cave_server_wait")
         return True
+
+    def progress(self, rid) -> RequestProgress:
+        """Simulations of the request that have reported, and their categories so far."""
+        p = RequestProgress()
+        self.ctx.check(lib().cave_server_progress(self.h, rid, ctypes.byref(p)), "cave_server_progress")
+        return p
 
     def cancel(self, rid):
         """Cancels a request: queued simulations leave the queue, running ones finish unreported."""

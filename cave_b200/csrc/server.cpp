@@ -43,6 +43,7 @@ struct Request {
     bool complete = false;
     bool cancelled = false;  // cave_server_cancel: results are dropped as they arrive
     bool expired = false;    // past the deadline: results are dropped, wait / fetch time out
+    uint64_t cat[3] = {0, 0, 0};  // categories of the results so far (viable, possible, unviable)
 };
 
 }  // namespace
@@ -123,6 +124,7 @@ static void server_loop(cave_server* s) {
             }
             q.results[ix] = r.result;
             q.results[ix].params = q.params[ix];
+            q.cat[std::min<uint32_t>(r.result.category, 2u)]++;
             q.done++;
             s->sims_completed++;
             s->outstanding--;
@@ -331,6 +333,24 @@ cave_status cave_server_fetch(cave_server* s, uint64_t requestId, cave_sim_resul
     for (uint64_t i = 0; i < n; i++) err |= out[i].error;
     if (err & kErrBounds) return set_error(s->ctx, CAVE_ERR_INTERNAL, "a served simulation failed an index check");
     if (err) return set_error(s->ctx, CAVE_ERR_TIMEOUT, "a served simulation raised a device error flag");
+    return CAVE_OK;
+}
+
+cave_status cave_server_progress(cave_server* s, uint64_t requestId, cave_request_progress* out) {
+    if (!s || !out) return CAVE_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->requests.find(requestId);
+    if (it == s->requests.end() || it->second.cancelled) return CAVE_ERR_INVALID_ARG;
+    const Request& q = it->second;
+    cave_request_progress p{};
+    p.total = q.n;
+    p.done = q.done;
+    p.viable = q.cat[0];
+    p.possible = q.cat[1];
+    p.unviable = q.cat[2];
+    p.complete = q.complete ? 1u : 0u;
+    p.expired = q.expired ? 1u : 0u;
+    *out = p;
     return CAVE_OK;
 }
 

@@ -405,6 +405,17 @@ cave_status cave_server_fetch(cave_server* s, uint64_t requestId, cave_sim_resul
                               double* latencySeconds);
 cave_status cave_server_get_stats(cave_server* s, cave_server_stats* out);
 
+/* Progress of one request (the reference's SearchProgress, searchSystem.h:29-38, per request):
+ * its simulations, how many have reported, and their categories so far. */
+typedef struct {
+    uint64_t total, done;
+    uint64_t viable, possible, unviable;
+    uint32_t complete;       /* all simulations reported                                  */
+    uint32_t expired;        /* passed requestDeadlineSeconds                             */
+} cave_request_progress;
+/* Non-blocking. CAVE_ERR_INVALID_ARG for an unknown (fetched, cancelled) request. */
+cave_status cave_server_progress(cave_server* s, uint64_t requestId, cave_request_progress* out);
+
 /* ---- render-mode cell buffers ---------------------------------------------------------- */
 /* Render mode keeps its cells in a different layout (cellStateUtils.slang:18-54, buffer mode):
  * two cells per texel along x (low nibble = even x), one texel per uint32 element, texels in

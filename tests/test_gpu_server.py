@@ -263,3 +263,26 @@ def test_injected_scheduler_failure_reaches_every_waiter(ctx, monkeypatch):
     res = run_alone(ctx, req, hbm_budget=1 << 30)
     for i in range(req.size):
         assert as_tuple(res[i]) == oracle_result(req[i]), f"sim {i}"
+
+
+def test_progress_counts_results_as_they_arrive(ctx):
+    """cave_server_progress (SearchProgress per request): done rises to the request's size, the
+    categories so far add up to it and, at the end, equal the fetched results'."""
+    req = long_request(24, edge=64, ticks=60)
+    with cb.Server(ctx, hbm_budget=1 << 30, max_active_cells=1, ticks_per_round=1) as s:
+        rid = s.submit(req)
+        seen = []
+        while True:
+            p = s.progress(rid)
+            assert p.total == req.size and p.viable + p.possible + p.unviable == p.done
+            seen.append(p.done)
+            if p.complete:
+                break
+            time.sleep(0.002)
+        assert seen == sorted(seen) and seen[-1] == req.size and not p.expired
+        res, _ = s.fetch(rid)
+        cats = np.bincount(np.asarray(res["category"], dtype=np.int64), minlength=3)
+        assert (p.viable, p.possible, p.unviable) == tuple(int(c) for c in cats)
+        with pytest.raises(cb.CaveError) as e:  # fetched: the id is released
+            s.progress(rid)
+        assert e.value.code == cb.ERR_INVALID_ARG
