@@ -57,3 +57,34 @@ def test_oracle_equals_vectorised_restatement(X, Y, Z, flags, maxcs, birth, surv
         assert tuple(stats.bbox_max) == tuple(int(v) for v in nz.max(axis=0)[::-1])
     else:
         assert tuple(stats.bbox_min) == (0xFFFFFFFF,) * 3 and tuple(stats.bbox_max) == (0, 0, 0)
+
+
+def numpy_run(s, maxcs, flags, birth, survival, max_ticks):
+    """searchManager.slang:115-139 over numpy_tick until the status is non-zero; GridInfo as
+    (totalDied, totalBorn, ticks, status, maxAlive, finalAlive) and the category of
+    searchSystem.cpp:697-711 (0 viable, 1 possible, 2 unviable)."""
+    died = born = ticks = max_alive = final = status = 0
+    while status == 0:
+        s, (dead, _, b, surv) = numpy_tick(s, maxcs, flags, birth, survival)
+        ticks += 1
+        died += dead
+        born += b
+        final = surv
+        max_alive = max(max_alive, surv)
+        status = 1 if surv == 0 and b == 0 else 2 if ticks >= max_ticks else 0
+    category = 0 if status == 2 else 1 if ticks > maxcs + 1 else 2
+    return (died, born, ticks, status, max_alive, final), category
+
+
+@settings(max_examples=100, deadline=None)
+@given(E=st.integers(2, 9), flags=st.integers(1, 7), maxcs=st.integers(1, 6), birth=st.integers(1, (1 << 26) - 1),
+       survival=st.integers(0, (1 << 26) - 1), max_ticks=st.integers(1, 12), seed=st.integers(0, 2 ** 31 - 1))
+def test_oracle_lifecycle_equals_restatement(E, flags, maxcs, birth, survival, max_ticks, seed):
+    """A rule's whole lifecycle (step until the manager stops it): GridInfo and category."""
+    rng = np.random.default_rng(seed)
+    s = np.where(rng.random((E, E, E)) < 0.35, maxcs, 0).astype(np.uint8)
+    params = O.make_params(maxcs, flags, birth, survival)
+    info, _, _ = O.run_sim(E, E, E, params, O.pack(s), max_ticks)
+    want_info, want_cat = numpy_run(s, maxcs, flags, birth, survival, max_ticks)
+    assert info.as_tuple() == want_info
+    assert O.classify(info, maxcs) == want_cat
