@@ -88,3 +88,46 @@ def test_oracle_lifecycle_equals_restatement(E, flags, maxcs, birth, survival, m
     want_info, want_cat = numpy_run(s, maxcs, flags, birth, survival, max_ticks)
     assert info.as_tuple() == want_info
     assert O.classify(info, maxcs) == want_cat
+
+
+def numpy_seed(X, Y, Z, spawn, size_index, random, density_index, run_seed, maxcs):
+    """The initial cells of searchSystem.cpp:219-306 (cube layout), vectorised: the spawn box
+    centred in the grid (scaled by the size index), cells inside it alive when the cell hash is
+    below the density threshold (or always when the spawn is filled), packed 8 per word."""
+    def dim(axis, d):
+        if size_index == 0:
+            return axis
+        return max(1, min(axis, (axis * (size_index + 1) + 15) // 16))
+
+    ex, ey, ez = (dim(min(s, d), d) for s, d in zip(spawn, (X, Y, Z)))
+    density = np.float32(density_index + 1) / np.float32(16)
+    threshold = 0xFFFFFFFF if density >= 1 else int(np.float64(density) * 4294967296.0)
+
+    def wang(v):
+        v = (v ^ np.uint32(61)) ^ (v >> np.uint32(16))
+        v = v * np.uint32(9)
+        v = v ^ (v >> np.uint32(4))
+        v = v * np.uint32(0x27D4EB2D)
+        return v ^ (v >> np.uint32(15))
+
+    z, y, x = np.meshgrid(np.arange(Z, dtype=np.uint32), np.arange(Y, dtype=np.uint32),
+                          np.arange(X, dtype=np.uint32), indexing="ij")
+    with np.errstate(over="ignore"):
+        h = wang(x * np.uint32(73856093) + np.uint32(run_seed))
+        h = wang(h ^ (y * np.uint32(19349663)))
+        h = wang(h ^ (z * np.uint32(83492791)))
+    inside = ((x >= (X - ex) // 2) & (x < (X + ex) // 2) & (y >= (Y - ey) // 2) & (y < (Y + ey) // 2) &
+              (z >= (Z - ez) // 2) & (z < (Z + ez) // 2))
+    alive = inside & ((density >= 1) | (h < np.uint32(threshold)) if random else inside)
+    return O.pack(np.where(alive, maxcs & 0xF, 0).astype(np.uint8))
+
+
+@settings(max_examples=100, deadline=None)
+@given(X=st.integers(1, 21), Y=st.integers(1, 11), Z=st.integers(1, 11), spawn=st.tuples(*[st.integers(1, 21)] * 3),
+       size_index=st.integers(0, 15), random=st.booleans(), density_index=st.integers(0, 15),
+       run_seed=st.integers(0, 2 ** 32 - 1), maxcs=st.integers(1, 16))
+def test_oracle_seed_equals_restatement(X, Y, Z, spawn, size_index, random, density_index, run_seed, maxcs):
+    got = O.seed(X, Y, Z, spawn=spawn, spawn_size_index=size_index, random=random,
+                 threshold=O.threshold_from_index(density_index), run_seed=run_seed, max_cell_state=maxcs)
+    want = numpy_seed(X, Y, Z, spawn, size_index, random, density_index, run_seed, maxcs)
+    assert np.array_equal(got, want)
