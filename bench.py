@@ -593,12 +593,17 @@ def sweep_workload(args, world, rank, local, pg, steps, warmup):
             b.results_array()
     barrier(pg, local)
     kern_ms, tot_ms, cats, ticks, launches, res = [], [], None, 0, 0, None
+    # the step's results land in pinned host memory (the end-to-end read-back)
+    import torch
+
+    pinned = torch.empty(full.size * cb.SIM_RESULT_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
+    out = pinned.numpy().view(cb.SIM_RESULT_DTYPE)
     with ClockSampler(local) as clk:
         for _ in range(steps):
             with make_batch() as b:
                 b.add_sims_array(full, max_rule_bits=2)
                 b.launch()
-                res = b.results_array()
+                res = b.results_array(out)
                 t = ctx.last_timing()
                 kern_ms.append(t.tick_ms)
                 tot_ms.append(t.total_ms)

@@ -552,10 +552,13 @@ class Batch:
         self.ctx.check(lib().cave_batch_add_sims(self.h, arr.ctypes.data_as(P(SimDesc)), arr.size, max_rule_bits),
                        "cave_batch_add_sims")
 
-    def results_array(self) -> np.ndarray:
-        """All results as a numpy array of dtype SIM_RESULT_DTYPE."""
+    def results_array(self, out: np.ndarray = None) -> np.ndarray:
+        """All results as a numpy array of dtype SIM_RESULT_DTYPE, written into `out` when given
+        (e.g. a view of pinned host memory, which the device writes at full link speed)."""
         n = lib().cave_batch_size(self.h)
-        out = np.zeros(max(n, 1), dtype=SIM_RESULT_DTYPE)
+        if out is None:
+            out = np.zeros(max(n, 1), dtype=SIM_RESULT_DTYPE)
+        assert out.dtype == SIM_RESULT_DTYPE and out.flags["C_CONTIGUOUS"] and out.size >= n
         self.ctx.check(lib().cave_batch_results(self.h, out.ctypes.data_as(P(SimResult)), n), "cave_batch_results")
         return out[:n]
 
