@@ -2,7 +2,8 @@
 run time built with -DCAVE_CHECKED): the hot kernels -- streaming (generic and rule-specialised,
 one and two ticks per launch) and resident -- test each shared- and global-memory index against
 the extent it must stay in, and a failed test skips the access and raises an error flag that the
-call returns as CAVE_ERR_INTERNAL. The parity suites of those kernels run in a child process on
+call returns as CAVE_ERR_INTERNAL. The engine's tiled tick kernels (one and two rows per thread)
+run under the same checks through the engine suite. The parity suites of those kernels run in a child process on
 the checked library: every result must equal the oracle's, so no check fired."""
 import os
 import subprocess
@@ -14,7 +15,7 @@ pytestmark = pytest.mark.gpu
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CHECKED = os.path.join(ROOT, "cave_b200", "libcave_ca_checked.so")
-SUITES = ["tests/test_gpu_parity.py", "tests/test_gpu_batch.py", "tests/test_gpu_jit.py"]
+SUITES = ["tests/test_gpu_parity.py", "tests/test_gpu_batch.py", "tests/test_gpu_jit.py", "tests/test_gpu_engine.py"]
 
 
 def test_parity_suites_pass_on_the_checked_library(tmp_path):
