@@ -558,7 +558,10 @@ class Batch:
         n = lib().cave_batch_size(self.h)
         if out is None:
             out = np.zeros(max(n, 1), dtype=SIM_RESULT_DTYPE)
-        assert out.dtype == SIM_RESULT_DTYPE and out.flags["C_CONTIGUOUS"] and out.size >= n
+        elif not (isinstance(out, np.ndarray) and out.dtype == SIM_RESULT_DTYPE and out.flags["C_CONTIGUOUS"]
+                  and out.flags["WRITEABLE"] and out.size >= n):
+            raise ValueError(f"results_array: out must be a writeable C-contiguous array of SIM_RESULT_DTYPE "
+                             f"with at least {n} elements")
         self.ctx.check(lib().cave_batch_results(self.h, out.ctypes.data_as(P(SimResult)), n), "cave_batch_results")
         return out[:n]
 

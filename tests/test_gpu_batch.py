@@ -117,6 +117,30 @@ def test_batch_device_seeded_inits(ctx):
         assert got(res[s]) == expected(G, G, G, O.make_params(3, 3, 0x60, 0x70), init, 20)
 
 
+
+def test_results_into_caller_memory(ctx):
+    """results_array(out): the same records written into a caller's array (here pinned host memory,
+    as the benchmark reads them); an array that is too small or of another dtype is refused before
+    the library writes anything."""
+    import torch
+
+    G = 49
+    thr = O.threshold_from_float(0.30)
+    with cb.Batch(ctx) as b:
+        ix = [b.add_init_seeded(G, G, G, (16, 16, 16), thr, s, 3) for s in range(5)]
+        b.add_sims([cb.SimDesc(cb.make_params(3, 3, 0x60, 0x70), ix[s], 20, 0, s) for s in range(5)])
+        b.launch()
+        ref = b.results_array().copy()
+        pinned = torch.empty(8 * cb.SIM_RESULT_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
+        out = pinned.numpy().view(cb.SIM_RESULT_DTYPE)
+        got_ = b.results_array(out)
+        assert got_.shape == (5,) and np.shares_memory(got_, out)
+        assert got_.tobytes() == ref.tobytes()
+        for bad in (np.zeros(4, dtype=cb.SIM_RESULT_DTYPE), np.zeros(8, dtype=np.uint64),
+                    np.zeros(16, dtype=cb.SIM_RESULT_DTYPE)[::2]):
+            with pytest.raises(ValueError):
+                b.results_array(bad)
+
 def test_withheld_initial_copy_times_out_without_a_fault(ctx, monkeypatch):
     """Failure path of the bounded device waits: with the failure test switch the resident
     kernel never issues a one-simulation batch's initial-grid copy, gives up its wait after 1 ms
