@@ -3,8 +3,8 @@
 ctypes bindings over ``oracle/cave_oracle.c`` (a plain-C restatement of the reference's
 shader and host arithmetic; see the header of that file for the reference lines it
 follows). Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
-may import this package, and only as the checker -- the product (``cave_b200``) never
-does.
+may import this package, and only to check results or as the timed CPU baseline -- the product
+(``cave_b200``) never does.
 """
 from __future__ import annotations
 

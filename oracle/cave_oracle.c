@@ -4,7 +4,7 @@
  * A plain-C restatement of CAVE's search-mode cellular-automaton arithmetic, used as
  * the parity oracle for the CUDA path and as the timed CPU baseline. Nothing in the
  * product (cave_b200/) links or calls this file; only tests/, __graft_entry__.smoke()
- * and bench.py's CPU-baseline leg load it, and only as the checker.
+ * and bench.py's CPU-baseline leg load it, and only to check results or to be timed.
  *
  * The reference has no CPU stepping (src/simulation/simulation.cpp:48-50: all cell
  * work happens in GPU shaders), so this file restates the shader and host arithmetic

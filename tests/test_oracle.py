@@ -1,4 +1,4 @@
-"""Known-answer and property tests of the CPU oracle (the parity checker).
+"""Known-answer and property tests of the CPU oracle (the parity reference).
 
 Hand-derived expectations follow the reference shader rules
 (shaders/slang/search/searchSimulationCube.slang:78-247, searchManager.slang:56-149,
