@@ -554,7 +554,8 @@ class Batch:
 
     def results_array(self, out: np.ndarray = None) -> np.ndarray:
         """All results as a numpy array of dtype SIM_RESULT_DTYPE, written into `out` when given
-        (e.g. a view of pinned host memory, which the device writes at full link speed)."""
+        (e.g. a view of pinned host memory, which the device writes at full link speed). Read the
+        results once per launch: simulations that ran tiled hand theirs over on the first read."""
         n = lib().cave_batch_size(self.h)
         if out is None:
             out = np.zeros(max(n, 1), dtype=SIM_RESULT_DTYPE)

@@ -314,7 +314,10 @@ cave_status cave_batch_launch(cave_batch* b);
 /* Non-blocking completion poll (the IsTickComplete of searchSystem.cpp:467-478): CAVE_OK
  * when the launched work has finished, CAVE_ERR_NOT_READY otherwise. */
 cave_status cave_batch_poll(cave_batch* b);
-/* Waits for the launched work and copies results (in queue order) to out[0..n). */
+/* Waits for the launched work and copies results (in queue order) to out[0..n). Call it once per
+ * launch: simulations that ran tiled hand their results over on the first call. `out` may be
+ * pageable or pinned host memory; pinned memory (cudaMallocHost) is written at full link speed,
+ * which matters for sweeps of millions of simulations (104 B per result). */
 cave_status cave_batch_results(cave_batch* b, cave_sim_result* out, uint64_t n);
 /* Simulations queued so far. */
 uint64_t cave_batch_size(const cave_batch* b);
