@@ -36,7 +36,7 @@ def numpy_tick(s, maxcs, flags, birth, survival):
     return new, counts
 
 
-@settings(max_examples=200, deadline=None)
+@settings(max_examples=1000, deadline=None)
 @given(X=st.integers(1, 19), Y=st.integers(1, 9), Z=st.integers(1, 9), flags=st.integers(0, 15),
        maxcs=st.integers(1, 16), birth=st.integers(0, (1 << 27) - 1), survival=st.integers(0, (1 << 27) - 1),
        p_alive=st.floats(0.0, 0.8), seed=st.integers(0, 2 ** 31 - 1))
@@ -76,7 +76,7 @@ def numpy_run(s, maxcs, flags, birth, survival, max_ticks):
     return (died, born, ticks, status, max_alive, final), category
 
 
-@settings(max_examples=100, deadline=None)
+@settings(max_examples=500, deadline=None)
 @given(E=st.integers(2, 9), flags=st.integers(1, 7), maxcs=st.integers(1, 6), birth=st.integers(1, (1 << 26) - 1),
        survival=st.integers(0, (1 << 26) - 1), max_ticks=st.integers(1, 12), seed=st.integers(0, 2 ** 31 - 1))
 def test_oracle_lifecycle_equals_restatement(E, flags, maxcs, birth, survival, max_ticks, seed):
@@ -122,7 +122,7 @@ def numpy_seed(X, Y, Z, spawn, size_index, random, density_index, run_seed, maxc
     return O.pack(np.where(alive, maxcs & 0xF, 0).astype(np.uint8))
 
 
-@settings(max_examples=100, deadline=None)
+@settings(max_examples=500, deadline=None)
 @given(X=st.integers(1, 21), Y=st.integers(1, 11), Z=st.integers(1, 11), spawn=st.tuples(*[st.integers(1, 21)] * 3),
        size_index=st.integers(0, 15), random=st.booleans(), density_index=st.integers(0, 15),
        run_seed=st.integers(0, 2 ** 32 - 1), maxcs=st.integers(1, 16))
