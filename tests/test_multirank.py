@@ -1,4 +1,4 @@
-"""The N > 1 path of bench.py on the CPU: two gloo ranks shard each workload (no collective on
+"""The N > 1 path of bench.py on the CPU: two and three gloo ranks shard each workload (no collective on
 the data path) and combine their timings with the max / sum reductions the GPU runs use. Every
 simulation must land on exactly one rank, and the reductions must see both ranks."""
 import datetime
@@ -37,10 +37,11 @@ def _worker(rank, world, port, out):
 
 
 @pytest.mark.timeout(180)
-def test_two_ranks_shard_without_overlap():
+@pytest.mark.parametrize("world", [2, 3])
+def test_ranks_shard_without_overlap(world):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    world, port = 2, _free_port()
+    port = _free_port()
     procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
     for p in procs:
         p.start()
@@ -54,11 +55,12 @@ def test_two_ranks_shard_without_overlap():
     import bench
 
     all_uneven = [s["seed"] for s in bench.uneven_sims(96)]
-    assert sorted(res[0][1] + res[1][1]) == sorted(all_uneven)
-    assert not set(res[0][1]) & set(res[1][1])
+    got_uneven = [v for r in res for v in r[1]]
+    assert sorted(got_uneven) == sorted(all_uneven) and len(set(got_uneven)) == len(got_uneven)
     all_sweep = [int(t) for t in bench.sweep_descs(49, 2, (2, 3))["tag"]]
-    assert sorted(res[0][2] + res[1][2]) == sorted(all_sweep)
-    assert len(res[0][3]) + len(res[1][3]) == 9
+    got_sweep = [v for r in res for v in r[2]]
+    assert sorted(got_sweep) == sorted(all_sweep) and len(set(got_sweep)) == len(got_sweep)
+    assert sum(len(r[3]) for r in res) == 9
     for r in res:
-        assert r[4] == 2.0                      # max over ranks
+        assert r[4] == float(world)             # max over ranks
         assert r[5] == len(all_uneven)          # sum over ranks
