@@ -105,3 +105,22 @@ def test_exit_while_compiling(tmp_path, wait_s):
     assert out.returncode == 0, out.stdout + out.stderr
     # the compile ran to completion before the exit: its cubin is in the cache
     assert any(f.endswith(".cubin") for f in os.listdir(tmp_path))
+
+
+def test_checked_library_compiles_its_kernels_under_their_own_key(tmp_path):
+    """The checked library compiles its rule-specialised kernels with -DCAVE_CHECKED (the bounds
+    checks of the streaming kernels) and caches them under a key of their own: the normal library
+    sharing the cache folder compiles its own cubin instead of loading the checked one."""
+    checked = os.path.join(ROOT, "cave_b200", "libcave_ca_checked.so")
+    if not os.path.exists(checked):
+        pytest.skip("build it with python -m cave_b200.build --checked")
+    cache = tmp_path / "jit"
+    code = ("import sys, cave_b200 as cb, oracle as O; "
+            "p = cb.SimParams(*[int(v) for v in O.make_params(15, 0x7, 0x10, 0x18)]); "
+            "ok, log = cb.jit_compile(p); print(log[-2000:]); sys.exit(0 if ok else 1)")
+    for lib in (checked, cb.LIB_PATH):
+        env = dict(os.environ, CAVE_LIB=lib, CAVE_JIT_CACHE=str(cache))
+        r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True,
+                           timeout=600)
+        assert r.returncode == 0, r.stdout + r.stderr
+    assert len([f for f in os.listdir(cache) if f.endswith(".cubin")]) == 2
