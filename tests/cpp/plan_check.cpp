@@ -7,6 +7,10 @@
 //  * the items cover every (y, z) of the grid exactly once, with in-range y and z ranges,
 //    and each carries the item count of its simulation in dir_items >> 1;
 //  * the tile's dynamic shared memory (the kernels' own size functions) fits one CTA (227 KB).
+// And the resident kernel's geometry (cave::resident_geometry, engine.cpp) for every grid that
+// resident_fits accepts, with and without a z-segment hint: whole warps of at most 1024 threads
+// covering nseg segments of Y * SXp lanes, segments covering every plane, shared memory within
+// the resident cap, and at least one CTA per SM.
 // Built with nvcc (the size functions sit in the kernels' headers); needs no GPU. Exit status
 // 0 = every check held.
 #include <cstdint>
@@ -51,6 +55,26 @@ int check(uint32_t X, uint32_t Y, uint32_t Z, uint32_t target, uint32_t hint, ui
     }
     return 0;
 }
+int check_resident(uint32_t X, uint32_t Y, uint32_t Z, uint32_t hint) {
+    if (!cave::resident_fits(X, Y, Z)) return 0;
+    uint32_t threads = 0;
+    const cave::ResLaunch P = cave::resident_geometry(X, Y, Z, hint, threads);
+    uint32_t sxp = 1;
+    while (sxp < (X + 31) / 32) sxp <<= 1;
+    const uint32_t cols = Y * sxp;
+    const bool ok = P.X == X && P.Y == Y && P.Z == Z && P.SX == (X + 31) / 32 && (1u << P.sxp_log2) == sxp &&
+                    P.nseg >= 1 && P.nseg <= Z && (hint == 0 || P.nseg <= hint) &&
+                    (uint64_t)P.seg_len * P.nseg >= Z && P.seg_len >= 1 && threads % 32 == 0 &&
+                    threads >= P.nseg * cols && threads < P.nseg * cols + 32 && threads <= 1024 &&
+                    cave::resident_smem_bytes(X, Y, Z, P.nseg) <= 220u * 1024u &&
+                    cave::resident_ctas_per_sm(P, threads) >= 1;
+    if (!ok) {
+        std::printf("bad resident geometry %u %u %u hint %u: nseg %u seg_len %u threads %u\n", X, Y, Z, hint, P.nseg,
+                    P.seg_len, threads);
+        return 1;
+    }
+    return 0;
+}
 }  // namespace
 
 int main() {
@@ -71,6 +95,15 @@ int main() {
         const uint32_t hint = rng() % 3 == 0 ? 0u : 1u + rng() % 1200;
         if (check(X, Y, Z, targets[rng() % 5], hint, spt, halo)) return 1;
     }
-    std::printf("ok %d plans\n", n);
+    int nres = 0;
+    for (uint32_t X : {1u, 8u, 25u, 33u, 49u, 64u, 65u, 97u, 128u})
+        for (uint32_t Y = 1; Y <= 130; Y += 3)
+            for (uint32_t Z = 1; Z <= 130; Z += 7)
+                for (uint32_t hint : {0u, 1u, 3u, 64u}) {
+                    if (check_resident(X, Y, Z, hint)) return 1;
+                    nres += cave::resident_fits(X, Y, Z) ? 1 : 0;
+                }
+    if (nres == 0) return 1;
+    std::printf("ok %d plans, %d resident geometries\n", n, nres);
     return 0;
 }

@@ -4,7 +4,8 @@ tests/cpp/plan_check.cpp is compiled with nvcc (host code; the kernels' shared-m
 functions come from their headers), linked with libcave_ca.so and run. No GPU needed. Checked:
 strips per row, whole warps within the kernel's thread limit, tiles within the CTA's rows,
 every (y, z) of the grid covered by exactly one work item, and the tile's shared memory within
-one CTA's 227 KB."""
+one CTA's 227 KB. The same program checks the resident kernel's geometry (z-segments, threads,
+shared memory, CTAs per SM) for every grid that fits shared memory in a 23,000-shape sweep."""
 import os
 import shutil
 import subprocess
@@ -17,7 +18,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 
 
-def test_stream_plans_cover_the_grid_within_the_kernel_limits(tmp_path):
+def test_stream_plans_and_resident_geometry_within_the_kernel_limits(tmp_path):
     nvcc = os.path.join(CUDA_HOME, "bin", "nvcc")
     if not os.path.exists(nvcc):
         nvcc = shutil.which("nvcc")
@@ -31,5 +32,6 @@ def test_stream_plans_cover_the_grid_within_the_kernel_limits(tmp_path):
                         "-o", str(exe), "-L", lib_dir, "-l:" + os.path.basename(cb.LIB_PATH),
                         "-Xlinker", "-rpath", "-Xlinker", lib_dir], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-3000:]
-    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    env = {k: v for k, v in os.environ.items() if k != "CAVE_RESIDENT_NSEG"}  # the default geometry rule
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300, env=env)
     assert r.returncode == 0 and r.stdout.strip().startswith("ok"), r.stdout[-2000:] + r.stderr[-2000:]
