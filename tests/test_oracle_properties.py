@@ -131,3 +131,35 @@ def test_oracle_seed_equals_restatement(X, Y, Z, spawn, size_index, random, dens
                  threshold=O.threshold_from_index(density_index), run_seed=run_seed, max_cell_state=maxcs)
     want = numpy_seed(X, Y, Z, spawn, size_index, random, density_index, run_seed, maxcs)
     assert np.array_equal(got, want)
+
+
+@settings(max_examples=300, deadline=None)
+@given(G=st.integers(3, 8), flags=st.integers(1, 7), maxcs=st.integers(1, 4), kindex=st.booleans(),
+       b0=st.integers(1, 6), s0=st.integers(1, 4), maxp=st.integers(1, 6), s_extra=st.integers(0, 2),
+       max_ticks=st.integers(1, 8), seed=st.integers(0, 1000))
+def test_slot_pipeline_walks_next_permutation_in_order(G, flags, maxcs, kindex, b0, s0, maxp, s_extra, max_ticks,
+                                                       seed):
+    """The literal SearchSystem slot (oracle_run_slot: reset, tick, manager and host read-back of
+    searchSystem.cpp:480-713 with NextPermutation, searchManager.slang:56-96) reports exactly the
+    rules of the permutation walk -- birth index from its start to maxPermutation, then the next
+    survival index with birth 1, up to survivalEnd -- in that order, once each, and each with the
+    result of running that rule alone from the initial cells."""
+    b0 = min(b0, maxp)
+    s_end = s0 + s_extra
+    valid = O.valid_bitmasks(6, 2) if kindex else None
+    init = O.seed(G, G, G, spawn=(G // 2 + 1,) * 3, random=True, threshold=1 << 31, run_seed=seed,
+                  max_cell_state=maxcs)
+    res = O.run_slot(G, G, G, ((maxcs - 1) << 60) | b0, (flags << 60) | s0, maxp, s_end, init, max_ticks,
+                     valid=valid, max_rule_bits=2 if kindex else 0)
+    walk = [(s0, b) for b in range(b0, maxp + 1)] + [(s, b) for s in range(s0 + 1, s_end + 1)
+                                                      for b in range(1, maxp + 1)]
+    assert len(res) == len(walk)
+    for r, (s, b) in zip(res, walk):
+        bm = int(valid[b - 1]) if kindex else b
+        sm = int(valid[s - 1]) if kindex else s
+        assert r.birthAndMaxCellStateRules == ((maxcs - 1) << 60) | bm
+        assert r.survivalAndNeighborhoodRules == (flags << 60) | sm
+        p = O.make_params(maxcs, flags, bm, sm)
+        info, _, _ = O.run_sim(G, G, G, p, init, max_ticks)
+        assert r.info.as_tuple() == info.as_tuple()
+        assert r.category == O.classify(info, maxcs)
