@@ -1,6 +1,10 @@
 """Rule strings (guiSystem.cpp:92-163), pinned by the reference's only exact-value test,
-`--test cli-rules` (testRunner.cpp:231-260): "3,5-7" and "2,4" round-trip, maxCS 8 decodes."""
+`--test cli-rules` (testRunner.cpp:231-260): "3,5-7" and "2,4" round-trip, maxCS 8 decodes; the
+parser's edge forms; and, on hypothesis-drawn masks, the formatter against a restatement of
+BitmaskToRuleString and the parse of its output back to the mask."""
 import pytest
+from hypothesis import given, settings
+from hypothesis import strategies as st
 
 import cave_b200 as cb
 
@@ -28,3 +32,28 @@ def test_cli_rules_known_answer():
 def test_rule_string_forms(text, mask, back):
     assert cb.rule_string_to_bitmask(text) == mask
     assert cb.bitmask_to_rule_string(mask) == back
+
+
+def _format(mask):
+    """guiSystem.cpp:92-123 restated: 1-based set bits below 60, runs of three or more as a-b."""
+    bits = [b + 1 for b in range(60) if (mask >> b) & 1]
+    if not bits:
+        return "-"
+    parts, i = [], 0
+    while i < len(bits):
+        j = i
+        while j + 1 < len(bits) and bits[j + 1] == bits[j] + 1:
+            j += 1
+        parts += [f"{bits[i]}-{bits[j]}"] if j - i >= 2 else [str(b) for b in bits[i:j + 1]]
+        i = j + 1
+    return ",".join(parts)
+
+
+
+@settings(max_examples=500, deadline=None)
+@given(mask=st.one_of(st.integers(0, (1 << 64) - 1), st.integers(0, (1 << 27) - 1),
+                      st.lists(st.integers(0, 59), max_size=8).map(lambda v: sum(1 << b for b in set(v)))))
+def test_rule_string_round_trip(mask):
+    text = cb.bitmask_to_rule_string(mask)
+    assert text == _format(mask)
+    assert cb.rule_string_to_bitmask(text) == (mask & ((1 << 60) - 1) if text != "-" else 0)
